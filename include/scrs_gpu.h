@@ -1,0 +1,318 @@
+/*
+ * scrs_gpu.h — C ABI of the B200 (sm_100a) erasure-coding engines.
+ *
+ * The surface mirrors the SCRS Rust trait family one-to-one so that a Rust
+ * (or any FFI) caller can drop the GPU engines in beside the CPU ones:
+ *
+ *   Profile::resolve / Profile::recommended      scrs/src/selector.rs:40,67
+ *   recommended_gf16_engine                      scrs/src/lib.rs:85
+ *   batch_encoder + BatchEncoder                 scrs/src/selector.rs:457, codec.rs:136-151
+ *   batch_decoder + BatchDecoder                 scrs/src/selector.rs:270, codec.rs:157-175
+ *   incremental_encoder + IncrementalEncoder     scrs/src/selector.rs:370, codec.rs:122-131
+ *   decoder + Decoder + SymbolSink               scrs/src/selector.rs:117, codec.rs:180-201,
+ *                                                scrs/src/transport/symbol_sink.rs:36-54
+ *   ConfigError / EncodeError / DecodeError      scrs/src/error.rs:12-126
+ *
+ * Conventions
+ *  - Every fallible call returns an int32 status: SCRS_OK (0) or one of the
+ *    SCRS_* codes below.  When `err` is non-NULL it receives the code and
+ *    the variant's detail fields (see scrs_error).
+ *  - Buffers passed to the plain entry points are HOST memory; the library
+ *    copies them to the device, runs the kernels and copies results back
+ *    before returning.  The *_device entry points take device pointers and
+ *    a CUDA stream (passed as void*) and return after enqueueing the work.
+ *  - Handles own their device memory.  After *_create / *_scratch, the
+ *    *_with calls perform no device or host allocation (the contract of
+ *    scrs/tests/zero_alloc.rs:103-145).
+ *  - Handles are not thread safe, as the reference engines are &mut-exclusive.
+ *  - Sizes are uint64_t; indices are uint64_t codeword positions.
+ */
+#ifndef SCRS_GPU_H
+#define SCRS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- vocabulary: scrs/src/codec.rs:20-39 ------------------------------ */
+enum {
+    SCRS_ENGINE_STANDARD_CAUCHY = 0, /* GF(256), k+m <= 256            */
+    SCRS_ENGINE_GOOD_CAUCHY = 1,     /* GF(256), k+m <= 255            */
+    SCRS_ENGINE_TOWER = 2,           /* GF((2^8)^2), k+m <= 65535      */
+    SCRS_ENGINE_AFFT = 3             /* GF(2^16) additive FFT, <= 65536 */
+};
+enum { SCRS_FIELD_GF256 = 0, SCRS_FIELD_GF65536 = 1 };
+
+/* ---- status codes: scrs/src/error.rs ----------------------------------- */
+enum {
+    SCRS_OK = 0,
+    /* ConfigError (error.rs:12-31); detail a = cap / engine */
+    SCRS_CONFIG_ZERO_DIMENSION = 101,
+    SCRS_CONFIG_TOO_MANY_SYMBOLS = 102, /* a = cap                        */
+    SCRS_CONFIG_ZERO_SYMBOL_LEN = 103,
+    SCRS_CONFIG_ODD_SYMBOL_LEN = 104,
+    SCRS_CONFIG_UNSUPPORTED_MODE = 105, /* a = engine                     */
+    /* EncodeError (error.rs:35-71) */
+    SCRS_ENCODE_WRONG_INPUT_LEN = 201,    /* a = expected, b = got        */
+    SCRS_ENCODE_INDEX_OUT_OF_RANGE = 202, /* a = index, b = n             */
+    SCRS_ENCODE_WRONG_PAYLOAD_LEN = 203,  /* a = expected, b = got        */
+    SCRS_ENCODE_DUPLICATE_DATA = 204,     /* a = index                    */
+    SCRS_ENCODE_WRONG_OUTPUT_LEN = 205,   /* a = expected, b = got        */
+    SCRS_ENCODE_SCRATCH_MISMATCH = 206,
+    /* DecodeError (error.rs:75-126) */
+    SCRS_DECODE_WRONG_COUNT = 301,        /* a = expected, b = got        */
+    SCRS_DECODE_INDEX_OUT_OF_RANGE = 302, /* a = index, b = n             */
+    SCRS_DECODE_DUPLICATE_INDEX = 303,    /* a = index                    */
+    SCRS_DECODE_WRONG_PAYLOAD_LEN = 304,  /* a = expected, b = got        */
+    SCRS_DECODE_TOO_MANY_SYMBOLS = 305,   /* a = cap, b = received        */
+    SCRS_DECODE_INSUFFICIENT_RANK = 306,  /* a = rank, b = k              */
+    SCRS_DECODE_WRONG_OUTPUT_LEN = 307,   /* a = expected, b = got        */
+    SCRS_DECODE_SCRATCH_MISMATCH = 308,
+    /* Runtime errors with no counterpart in the reference (a CPU library
+     * cannot meet them): bad pointers, CUDA failures, device limits. */
+    SCRS_ERR_NULL_ARGUMENT = 901,
+    SCRS_ERR_CUDA = 902,          /* a = cudaError_t value                 */
+    SCRS_ERR_OUT_OF_MEMORY = 903, /* a = bytes requested                   */
+    SCRS_ERR_NO_DEVICE = 904,
+    SCRS_ERR_CAPACITY = 905,      /* a = requested, b = limit              */
+    SCRS_ERR_DEVICE_TIMEOUT = 906,/* a bounded device-side wait expired    */
+    SCRS_ERR_BAD_ARGUMENT = 907   /* a = argument position                 */
+};
+
+/* PushOutcome (symbol_sink.rs:11-26) */
+enum { SCRS_PUSH_ADVANCED = 0, SCRS_PUSH_COMPLETE = 1, SCRS_PUSH_DEPENDENT = 2 };
+
+typedef struct scrs_profile {
+    int32_t engine;
+    int32_t reserved;
+    uint64_t k;
+    uint64_t m;
+    uint64_t symbol_len;
+} scrs_profile;
+
+typedef struct scrs_error {
+    int32_t code;
+    int32_t reserved;
+    uint64_t a;
+    uint64_t b;
+} scrs_error;
+
+typedef struct scrs_push_outcome {
+    int32_t kind; /* SCRS_PUSH_* */
+    int32_t reserved;
+    uint64_t rank;     /* valid for SCRS_PUSH_ADVANCED */
+    uint64_t received; /* valid for SCRS_PUSH_ADVANCED */
+} scrs_push_outcome;
+
+typedef struct scrs_batch_encoder scrs_batch_encoder;
+typedef struct scrs_encode_scratch scrs_encode_scratch;
+typedef struct scrs_batch_decoder scrs_batch_decoder;
+typedef struct scrs_batch_decode_scratch scrs_batch_decode_scratch;
+typedef struct scrs_incremental_encoder scrs_incremental_encoder;
+typedef struct scrs_decoder scrs_decoder;
+typedef struct scrs_decode_scratch scrs_decode_scratch;
+typedef struct scrs_stripe_batch scrs_stripe_batch;
+
+/* ---- library ------------------------------------------------------------ */
+/* ABI version (major << 16 | minor). No reference counterpart. */
+uint32_t scrs_abi_version(void);
+/* Human-readable name of a status code. No reference counterpart. */
+const char* scrs_status_name(int32_t code);
+
+/* ---- profiles: selector.rs:40-88, lib.rs:85-93 -------------------------- */
+int32_t scrs_profile_resolve(int32_t engine, uint64_t k, uint64_t m,
+                             uint64_t symbol_len, scrs_profile* out,
+                             scrs_error* err);
+int32_t scrs_profile_recommended(int32_t field, uint64_t k, uint64_t m,
+                                 uint64_t symbol_len, scrs_profile* out,
+                                 scrs_error* err);
+/* Returns SCRS_ENGINE_TOWER or SCRS_ENGINE_AFFT (lib.rs:85). */
+int32_t scrs_recommended_gf16_engine(uint64_t k, uint64_t m);
+
+/* ---- BatchEncoder: selector.rs:457-529, codec.rs:136-151 ---------------- */
+/* UnsupportedMode for Tower (selector.rs:465). */
+int32_t scrs_batch_encoder_create(const scrs_profile* profile,
+                                  scrs_batch_encoder** out, scrs_error* err);
+void scrs_batch_encoder_destroy(scrs_batch_encoder* enc);
+int32_t scrs_batch_encoder_profile(const scrs_batch_encoder* enc,
+                                   scrs_profile* out);
+/* BatchEncoder::scratch (codec.rs:140). */
+int32_t scrs_batch_encoder_scratch(const scrs_batch_encoder* enc,
+                                   scrs_encode_scratch** out, scrs_error* err);
+void scrs_encode_scratch_destroy(scrs_encode_scratch* scratch);
+/* BatchEncoder::encode_into (codec.rs:143): throwaway scratch. */
+int32_t scrs_batch_encode_into(const scrs_batch_encoder* enc,
+                               const uint8_t* data, uint64_t data_len,
+                               uint8_t* repairs, uint64_t repairs_len,
+                               scrs_error* err);
+/* BatchEncoder::encode_into_with (codec.rs:145): host buffers. */
+int32_t scrs_batch_encode_into_with(const scrs_batch_encoder* enc,
+                                    const uint8_t* data, uint64_t data_len,
+                                    uint8_t* repairs, uint64_t repairs_len,
+                                    scrs_encode_scratch* scratch,
+                                    scrs_error* err);
+/* Device-resident form of encode_into_with: d_data / d_repairs are device
+ * pointers; enqueued on `stream` (a cudaStream_t, NULL = legacy default). */
+int32_t scrs_batch_encode_into_with_device(const scrs_batch_encoder* enc,
+                                           const uint8_t* d_data,
+                                           uint64_t data_len,
+                                           uint8_t* d_repairs,
+                                           uint64_t repairs_len,
+                                           scrs_encode_scratch* scratch,
+                                           void* stream, scrs_error* err);
+
+/* ---- BatchDecoder: selector.rs:270-352, codec.rs:157-175 ---------------- */
+int32_t scrs_batch_decoder_create(const scrs_profile* profile,
+                                  scrs_batch_decoder** out, scrs_error* err);
+void scrs_batch_decoder_destroy(scrs_batch_decoder* dec);
+int32_t scrs_batch_decoder_profile(const scrs_batch_decoder* dec,
+                                   scrs_profile* out);
+int32_t scrs_batch_decoder_scratch(const scrs_batch_decoder* dec,
+                                   scrs_batch_decode_scratch** out,
+                                   scrs_error* err);
+void scrs_batch_decode_scratch_destroy(scrs_batch_decode_scratch* scratch);
+/* BatchDecoder::decode_into_with (codec.rs:169).  The Rust slice of
+ * (index, payload) pairs is passed as three parallel arrays of `count`
+ * entries: indices[i], payloads[i] (host pointer), payload_lens[i]. */
+int32_t scrs_batch_decode_into_with(scrs_batch_decoder* dec,
+                                    const uint64_t* indices,
+                                    const uint8_t* const* payloads,
+                                    const uint64_t* payload_lens,
+                                    uint64_t count, uint8_t* out,
+                                    uint64_t out_len,
+                                    scrs_batch_decode_scratch* scratch,
+                                    scrs_error* err);
+/* BatchDecoder::decode_into (codec.rs:163): throwaway scratch. */
+int32_t scrs_batch_decode_into(scrs_batch_decoder* dec,
+                               const uint64_t* indices,
+                               const uint8_t* const* payloads,
+                               const uint64_t* payload_lens, uint64_t count,
+                               uint8_t* out, uint64_t out_len,
+                               scrs_error* err);
+/* Device-resident form: payloads are `count` rows of symbol_len bytes at
+ * d_payloads (row i belongs to indices[i], indices in HOST memory); d_out is
+ * k*symbol_len device bytes. Enqueued on `stream`. */
+int32_t scrs_batch_decode_into_with_device(scrs_batch_decoder* dec,
+                                           const uint64_t* indices,
+                                           const uint8_t* d_payloads,
+                                           uint64_t count, uint8_t* d_out,
+                                           uint64_t out_len,
+                                           scrs_batch_decode_scratch* scratch,
+                                           void* stream, scrs_error* err);
+
+/* ---- IncrementalEncoder: selector.rs:370-429, codec.rs:122-131 ---------- */
+/* UnsupportedMode for Standard Cauchy and AFFT (selector.rs:379). */
+int32_t scrs_incremental_encoder_create(const scrs_profile* profile,
+                                        scrs_incremental_encoder** out,
+                                        scrs_error* err);
+void scrs_incremental_encoder_destroy(scrs_incremental_encoder* enc);
+int32_t scrs_incremental_encoder_profile(const scrs_incremental_encoder* enc,
+                                         scrs_profile* out);
+/* IncrementalEncoder::feed (codec.rs:124): host payload. */
+int32_t scrs_inc_feed(scrs_incremental_encoder* enc, uint64_t index,
+                      const uint8_t* data, uint64_t data_len,
+                      scrs_error* err);
+/* Device-resident feed: d_data is a device pointer; enqueued on the
+ * encoder's own stream (ordered with later calls on this handle). */
+int32_t scrs_inc_feed_device(scrs_incremental_encoder* enc, uint64_t index,
+                             const uint8_t* d_data, uint64_t data_len,
+                             scrs_error* err);
+/* IncrementalEncoder::repair (codec.rs:126).  The Rust call borrows the
+ * repair; across the ABI the repair is copied into `dst` (host). */
+int32_t scrs_inc_repair(const scrs_incremental_encoder* enc, uint64_t index,
+                        uint8_t* dst, uint64_t dst_len, scrs_error* err);
+/* Borrow form: device address of repair `index` (valid until destroy). */
+int32_t scrs_inc_repair_device(const scrs_incremental_encoder* enc,
+                               uint64_t index, const uint8_t** d_repair,
+                               scrs_error* err);
+uint64_t scrs_inc_fed_count(const scrs_incremental_encoder* enc);
+void scrs_inc_reset(scrs_incremental_encoder* enc);
+
+/* ---- Decoder + SymbolSink: selector.rs:117-242, codec.rs:180-201 -------- */
+int32_t scrs_decoder_create(const scrs_profile* profile, scrs_decoder** out,
+                            scrs_error* err);
+void scrs_decoder_destroy(scrs_decoder* dec);
+int32_t scrs_decoder_profile(const scrs_decoder* dec, scrs_profile* out);
+int32_t scrs_decoder_scratch(const scrs_decoder* dec,
+                             scrs_decode_scratch** out, scrs_error* err);
+void scrs_decode_scratch_destroy(scrs_decode_scratch* scratch);
+/* SymbolSink::push (symbol_sink.rs:42): host payload, copied to the
+ * device-resident payload buffer (no payload arithmetic). */
+int32_t scrs_dec_push(scrs_decoder* dec, uint64_t index,
+                      const uint8_t* payload, uint64_t payload_len,
+                      scrs_push_outcome* outcome, scrs_error* err);
+/* Device-resident push: d_payload is a device pointer. */
+int32_t scrs_dec_push_device(scrs_decoder* dec, uint64_t index,
+                             const uint8_t* d_payload, uint64_t payload_len,
+                             scrs_push_outcome* outcome, scrs_error* err);
+int32_t scrs_dec_is_complete(const scrs_decoder* dec);
+uint64_t scrs_dec_rank(const scrs_decoder* dec);
+uint64_t scrs_dec_received(const scrs_decoder* dec);
+void scrs_dec_reset(scrs_decoder* dec);
+/* Decoder::finalize_into (codec.rs:194): throwaway scratch. */
+int32_t scrs_dec_finalize_into(scrs_decoder* dec, uint8_t* out,
+                               uint64_t out_len, scrs_error* err);
+/* Decoder::finalize_into_with (codec.rs:196): host output. */
+int32_t scrs_dec_finalize_into_with(scrs_decoder* dec, uint8_t* out,
+                                    uint64_t out_len,
+                                    scrs_decode_scratch* scratch,
+                                    scrs_error* err);
+/* Device-resident finalize into d_out (device), enqueued on `stream`. */
+int32_t scrs_dec_finalize_into_with_device(scrs_decoder* dec, uint8_t* d_out,
+                                           uint64_t out_len,
+                                           scrs_decode_scratch* scratch,
+                                           void* stream, scrs_error* err);
+
+/* ---- Batched GF(256) stripes in one persistent launch ------------------
+ * No single reference counterpart: this runs many independent
+ * BatchCodec::encode_into (batch/codec.rs:156) and
+ * BatchCodec::decode_into_with (batch/codec.rs:278) calls of uneven
+ * geometry as one device work queue.  Per-stripe decode matrices are built
+ * on the device.  All pointers in a stripe descriptor are device pointers
+ * except `indices`, which is host memory read during submit. */
+enum { SCRS_OP_ENCODE = 0, SCRS_OP_DECODE = 1 };
+
+typedef struct scrs_stripe_desc {
+    int32_t op;     /* SCRS_OP_ENCODE or SCRS_OP_DECODE                     */
+    int32_t engine; /* SCRS_ENGINE_STANDARD_CAUCHY or SCRS_ENGINE_GOOD_CAUCHY */
+    uint32_t k;
+    uint32_t m;
+    uint64_t symbol_len;
+    /* encode: k*symbol_len data, row i at in + i*symbol_len.
+     * decode: k received symbols, row i at in + i*symbol_len. */
+    const uint8_t* in;
+    /* encode: m*symbol_len repairs.  decode: k*symbol_len data. */
+    uint8_t* out;
+    /* decode only: k codeword indices of the received rows (host memory). */
+    const uint16_t* indices;
+} scrs_stripe_desc;
+
+/* Capacity is fixed at creation so that submit allocates nothing. */
+int32_t scrs_stripe_batch_create(uint64_t max_stripes, uint64_t max_work_items,
+                                 scrs_stripe_batch** out, scrs_error* err);
+void scrs_stripe_batch_destroy(scrs_stripe_batch* batch);
+/* Validate and upload `count` descriptors (the host part of a submit).
+ * Errors carry the first offending stripe position in `err->b` when the
+ * variant has no second detail field. */
+int32_t scrs_stripe_batch_set(scrs_stripe_batch* batch,
+                              const scrs_stripe_desc* descs, uint64_t count,
+                              scrs_error* err);
+/* Run the uploaded stripes on `stream`: one device-side plan kernel builds
+ * every decode matrix, one persistent kernel drains the work queue.  With
+ * use_graph != 0 the pair is captured once into a CUDA graph and replayed. */
+int32_t scrs_stripe_batch_run(scrs_stripe_batch* batch, void* stream,
+                              int32_t use_graph, scrs_error* err);
+/* Baseline form of the same work: one plan launch and one kernel launch per
+ * stripe (the plain one-call-per-stripe GPU form). */
+int32_t scrs_stripe_batch_run_plain(scrs_stripe_batch* batch, void* stream,
+                                    scrs_error* err);
+/* Number of kernels the last run launched (for launch accounting). */
+uint64_t scrs_stripe_batch_last_launches(const scrs_stripe_batch* batch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SCRS_GPU_H */
