@@ -33,6 +33,12 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#if defined(__GNUC__)
+#define SCRS_API __attribute__((visibility("default")))
+#else
+#define SCRS_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -118,45 +124,45 @@ typedef struct scrs_stripe_batch scrs_stripe_batch;
 
 /* ---- library ------------------------------------------------------------ */
 /* ABI version (major << 16 | minor). No reference counterpart. */
-uint32_t scrs_abi_version(void);
+SCRS_API uint32_t scrs_abi_version(void);
 /* Human-readable name of a status code. No reference counterpart. */
-const char* scrs_status_name(int32_t code);
+SCRS_API const char* scrs_status_name(int32_t code);
 
 /* ---- profiles: selector.rs:40-88, lib.rs:85-93 -------------------------- */
-int32_t scrs_profile_resolve(int32_t engine, uint64_t k, uint64_t m,
+SCRS_API int32_t scrs_profile_resolve(int32_t engine, uint64_t k, uint64_t m,
                              uint64_t symbol_len, scrs_profile* out,
                              scrs_error* err);
-int32_t scrs_profile_recommended(int32_t field, uint64_t k, uint64_t m,
+SCRS_API int32_t scrs_profile_recommended(int32_t field, uint64_t k, uint64_t m,
                                  uint64_t symbol_len, scrs_profile* out,
                                  scrs_error* err);
 /* Returns SCRS_ENGINE_TOWER or SCRS_ENGINE_AFFT (lib.rs:85). */
-int32_t scrs_recommended_gf16_engine(uint64_t k, uint64_t m);
+SCRS_API int32_t scrs_recommended_gf16_engine(uint64_t k, uint64_t m);
 
 /* ---- BatchEncoder: selector.rs:457-529, codec.rs:136-151 ---------------- */
 /* UnsupportedMode for Tower (selector.rs:465). */
-int32_t scrs_batch_encoder_create(const scrs_profile* profile,
+SCRS_API int32_t scrs_batch_encoder_create(const scrs_profile* profile,
                                   scrs_batch_encoder** out, scrs_error* err);
-void scrs_batch_encoder_destroy(scrs_batch_encoder* enc);
-int32_t scrs_batch_encoder_profile(const scrs_batch_encoder* enc,
+SCRS_API void scrs_batch_encoder_destroy(scrs_batch_encoder* enc);
+SCRS_API int32_t scrs_batch_encoder_profile(const scrs_batch_encoder* enc,
                                    scrs_profile* out);
 /* BatchEncoder::scratch (codec.rs:140). */
-int32_t scrs_batch_encoder_scratch(const scrs_batch_encoder* enc,
+SCRS_API int32_t scrs_batch_encoder_scratch(const scrs_batch_encoder* enc,
                                    scrs_encode_scratch** out, scrs_error* err);
-void scrs_encode_scratch_destroy(scrs_encode_scratch* scratch);
+SCRS_API void scrs_encode_scratch_destroy(scrs_encode_scratch* scratch);
 /* BatchEncoder::encode_into (codec.rs:143): throwaway scratch. */
-int32_t scrs_batch_encode_into(const scrs_batch_encoder* enc,
+SCRS_API int32_t scrs_batch_encode_into(const scrs_batch_encoder* enc,
                                const uint8_t* data, uint64_t data_len,
                                uint8_t* repairs, uint64_t repairs_len,
                                scrs_error* err);
 /* BatchEncoder::encode_into_with (codec.rs:145): host buffers. */
-int32_t scrs_batch_encode_into_with(const scrs_batch_encoder* enc,
+SCRS_API int32_t scrs_batch_encode_into_with(const scrs_batch_encoder* enc,
                                     const uint8_t* data, uint64_t data_len,
                                     uint8_t* repairs, uint64_t repairs_len,
                                     scrs_encode_scratch* scratch,
                                     scrs_error* err);
 /* Device-resident form of encode_into_with: d_data / d_repairs are device
  * pointers; enqueued on `stream` (a cudaStream_t, NULL = legacy default). */
-int32_t scrs_batch_encode_into_with_device(const scrs_batch_encoder* enc,
+SCRS_API int32_t scrs_batch_encode_into_with_device(const scrs_batch_encoder* enc,
                                            const uint8_t* d_data,
                                            uint64_t data_len,
                                            uint8_t* d_repairs,
@@ -165,19 +171,19 @@ int32_t scrs_batch_encode_into_with_device(const scrs_batch_encoder* enc,
                                            void* stream, scrs_error* err);
 
 /* ---- BatchDecoder: selector.rs:270-352, codec.rs:157-175 ---------------- */
-int32_t scrs_batch_decoder_create(const scrs_profile* profile,
+SCRS_API int32_t scrs_batch_decoder_create(const scrs_profile* profile,
                                   scrs_batch_decoder** out, scrs_error* err);
-void scrs_batch_decoder_destroy(scrs_batch_decoder* dec);
-int32_t scrs_batch_decoder_profile(const scrs_batch_decoder* dec,
+SCRS_API void scrs_batch_decoder_destroy(scrs_batch_decoder* dec);
+SCRS_API int32_t scrs_batch_decoder_profile(const scrs_batch_decoder* dec,
                                    scrs_profile* out);
-int32_t scrs_batch_decoder_scratch(const scrs_batch_decoder* dec,
+SCRS_API int32_t scrs_batch_decoder_scratch(const scrs_batch_decoder* dec,
                                    scrs_batch_decode_scratch** out,
                                    scrs_error* err);
-void scrs_batch_decode_scratch_destroy(scrs_batch_decode_scratch* scratch);
+SCRS_API void scrs_batch_decode_scratch_destroy(scrs_batch_decode_scratch* scratch);
 /* BatchDecoder::decode_into_with (codec.rs:169).  The Rust slice of
  * (index, payload) pairs is passed as three parallel arrays of `count`
  * entries: indices[i], payloads[i] (host pointer), payload_lens[i]. */
-int32_t scrs_batch_decode_into_with(scrs_batch_decoder* dec,
+SCRS_API int32_t scrs_batch_decode_into_with(scrs_batch_decoder* dec,
                                     const uint64_t* indices,
                                     const uint8_t* const* payloads,
                                     const uint64_t* payload_lens,
@@ -186,7 +192,7 @@ int32_t scrs_batch_decode_into_with(scrs_batch_decoder* dec,
                                     scrs_batch_decode_scratch* scratch,
                                     scrs_error* err);
 /* BatchDecoder::decode_into (codec.rs:163): throwaway scratch. */
-int32_t scrs_batch_decode_into(scrs_batch_decoder* dec,
+SCRS_API int32_t scrs_batch_decode_into(scrs_batch_decoder* dec,
                                const uint64_t* indices,
                                const uint8_t* const* payloads,
                                const uint64_t* payload_lens, uint64_t count,
@@ -195,7 +201,7 @@ int32_t scrs_batch_decode_into(scrs_batch_decoder* dec,
 /* Device-resident form: payloads are `count` rows of symbol_len bytes at
  * d_payloads (row i belongs to indices[i], indices in HOST memory); d_out is
  * k*symbol_len device bytes. Enqueued on `stream`. */
-int32_t scrs_batch_decode_into_with_device(scrs_batch_decoder* dec,
+SCRS_API int32_t scrs_batch_decode_into_with_device(scrs_batch_decoder* dec,
                                            const uint64_t* indices,
                                            const uint8_t* d_payloads,
                                            uint64_t count, uint8_t* d_out,
@@ -205,63 +211,63 @@ int32_t scrs_batch_decode_into_with_device(scrs_batch_decoder* dec,
 
 /* ---- IncrementalEncoder: selector.rs:370-429, codec.rs:122-131 ---------- */
 /* UnsupportedMode for Standard Cauchy and AFFT (selector.rs:379). */
-int32_t scrs_incremental_encoder_create(const scrs_profile* profile,
+SCRS_API int32_t scrs_incremental_encoder_create(const scrs_profile* profile,
                                         scrs_incremental_encoder** out,
                                         scrs_error* err);
-void scrs_incremental_encoder_destroy(scrs_incremental_encoder* enc);
-int32_t scrs_incremental_encoder_profile(const scrs_incremental_encoder* enc,
+SCRS_API void scrs_incremental_encoder_destroy(scrs_incremental_encoder* enc);
+SCRS_API int32_t scrs_incremental_encoder_profile(const scrs_incremental_encoder* enc,
                                          scrs_profile* out);
 /* IncrementalEncoder::feed (codec.rs:124): host payload. */
-int32_t scrs_inc_feed(scrs_incremental_encoder* enc, uint64_t index,
+SCRS_API int32_t scrs_inc_feed(scrs_incremental_encoder* enc, uint64_t index,
                       const uint8_t* data, uint64_t data_len,
                       scrs_error* err);
 /* Device-resident feed: d_data is a device pointer; enqueued on the
  * encoder's own stream (ordered with later calls on this handle). */
-int32_t scrs_inc_feed_device(scrs_incremental_encoder* enc, uint64_t index,
+SCRS_API int32_t scrs_inc_feed_device(scrs_incremental_encoder* enc, uint64_t index,
                              const uint8_t* d_data, uint64_t data_len,
                              scrs_error* err);
 /* IncrementalEncoder::repair (codec.rs:126).  The Rust call borrows the
  * repair; across the ABI the repair is copied into `dst` (host). */
-int32_t scrs_inc_repair(const scrs_incremental_encoder* enc, uint64_t index,
+SCRS_API int32_t scrs_inc_repair(const scrs_incremental_encoder* enc, uint64_t index,
                         uint8_t* dst, uint64_t dst_len, scrs_error* err);
 /* Borrow form: device address of repair `index` (valid until destroy). */
-int32_t scrs_inc_repair_device(const scrs_incremental_encoder* enc,
+SCRS_API int32_t scrs_inc_repair_device(const scrs_incremental_encoder* enc,
                                uint64_t index, const uint8_t** d_repair,
                                scrs_error* err);
-uint64_t scrs_inc_fed_count(const scrs_incremental_encoder* enc);
-void scrs_inc_reset(scrs_incremental_encoder* enc);
+SCRS_API uint64_t scrs_inc_fed_count(const scrs_incremental_encoder* enc);
+SCRS_API void scrs_inc_reset(scrs_incremental_encoder* enc);
 
 /* ---- Decoder + SymbolSink: selector.rs:117-242, codec.rs:180-201 -------- */
-int32_t scrs_decoder_create(const scrs_profile* profile, scrs_decoder** out,
+SCRS_API int32_t scrs_decoder_create(const scrs_profile* profile, scrs_decoder** out,
                             scrs_error* err);
-void scrs_decoder_destroy(scrs_decoder* dec);
-int32_t scrs_decoder_profile(const scrs_decoder* dec, scrs_profile* out);
-int32_t scrs_decoder_scratch(const scrs_decoder* dec,
+SCRS_API void scrs_decoder_destroy(scrs_decoder* dec);
+SCRS_API int32_t scrs_decoder_profile(const scrs_decoder* dec, scrs_profile* out);
+SCRS_API int32_t scrs_decoder_scratch(const scrs_decoder* dec,
                              scrs_decode_scratch** out, scrs_error* err);
-void scrs_decode_scratch_destroy(scrs_decode_scratch* scratch);
+SCRS_API void scrs_decode_scratch_destroy(scrs_decode_scratch* scratch);
 /* SymbolSink::push (symbol_sink.rs:42): host payload, copied to the
  * device-resident payload buffer (no payload arithmetic). */
-int32_t scrs_dec_push(scrs_decoder* dec, uint64_t index,
+SCRS_API int32_t scrs_dec_push(scrs_decoder* dec, uint64_t index,
                       const uint8_t* payload, uint64_t payload_len,
                       scrs_push_outcome* outcome, scrs_error* err);
 /* Device-resident push: d_payload is a device pointer. */
-int32_t scrs_dec_push_device(scrs_decoder* dec, uint64_t index,
+SCRS_API int32_t scrs_dec_push_device(scrs_decoder* dec, uint64_t index,
                              const uint8_t* d_payload, uint64_t payload_len,
                              scrs_push_outcome* outcome, scrs_error* err);
-int32_t scrs_dec_is_complete(const scrs_decoder* dec);
-uint64_t scrs_dec_rank(const scrs_decoder* dec);
-uint64_t scrs_dec_received(const scrs_decoder* dec);
-void scrs_dec_reset(scrs_decoder* dec);
+SCRS_API int32_t scrs_dec_is_complete(const scrs_decoder* dec);
+SCRS_API uint64_t scrs_dec_rank(const scrs_decoder* dec);
+SCRS_API uint64_t scrs_dec_received(const scrs_decoder* dec);
+SCRS_API void scrs_dec_reset(scrs_decoder* dec);
 /* Decoder::finalize_into (codec.rs:194): throwaway scratch. */
-int32_t scrs_dec_finalize_into(scrs_decoder* dec, uint8_t* out,
+SCRS_API int32_t scrs_dec_finalize_into(scrs_decoder* dec, uint8_t* out,
                                uint64_t out_len, scrs_error* err);
 /* Decoder::finalize_into_with (codec.rs:196): host output. */
-int32_t scrs_dec_finalize_into_with(scrs_decoder* dec, uint8_t* out,
+SCRS_API int32_t scrs_dec_finalize_into_with(scrs_decoder* dec, uint8_t* out,
                                     uint64_t out_len,
                                     scrs_decode_scratch* scratch,
                                     scrs_error* err);
 /* Device-resident finalize into d_out (device), enqueued on `stream`. */
-int32_t scrs_dec_finalize_into_with_device(scrs_decoder* dec, uint8_t* d_out,
+SCRS_API int32_t scrs_dec_finalize_into_with_device(scrs_decoder* dec, uint8_t* d_out,
                                            uint64_t out_len,
                                            scrs_decode_scratch* scratch,
                                            void* stream, scrs_error* err);
@@ -291,26 +297,29 @@ typedef struct scrs_stripe_desc {
 } scrs_stripe_desc;
 
 /* Capacity is fixed at creation so that submit allocates nothing. */
-int32_t scrs_stripe_batch_create(uint64_t max_stripes, uint64_t max_work_items,
+SCRS_API int32_t scrs_stripe_batch_create(uint64_t max_stripes, uint64_t max_work_items,
                                  scrs_stripe_batch** out, scrs_error* err);
-void scrs_stripe_batch_destroy(scrs_stripe_batch* batch);
+SCRS_API void scrs_stripe_batch_destroy(scrs_stripe_batch* batch);
 /* Validate and upload `count` descriptors (the host part of a submit).
  * Errors carry the first offending stripe position in `err->b` when the
  * variant has no second detail field. */
-int32_t scrs_stripe_batch_set(scrs_stripe_batch* batch,
+SCRS_API int32_t scrs_stripe_batch_set(scrs_stripe_batch* batch,
                               const scrs_stripe_desc* descs, uint64_t count,
                               scrs_error* err);
 /* Run the uploaded stripes on `stream`: one device-side plan kernel builds
  * every decode matrix, one persistent kernel drains the work queue.  With
  * use_graph != 0 the pair is captured once into a CUDA graph and replayed. */
-int32_t scrs_stripe_batch_run(scrs_stripe_batch* batch, void* stream,
+SCRS_API int32_t scrs_stripe_batch_run(scrs_stripe_batch* batch, void* stream,
                               int32_t use_graph, scrs_error* err);
 /* Baseline form of the same work: one plan launch and one kernel launch per
  * stripe (the plain one-call-per-stripe GPU form). */
-int32_t scrs_stripe_batch_run_plain(scrs_stripe_batch* batch, void* stream,
+SCRS_API int32_t scrs_stripe_batch_run_plain(scrs_stripe_batch* batch, void* stream,
                                     scrs_error* err);
 /* Number of kernels the last run launched (for launch accounting). */
-uint64_t scrs_stripe_batch_last_launches(const scrs_stripe_batch* batch);
+SCRS_API uint64_t scrs_stripe_batch_last_launches(const scrs_stripe_batch* batch);
+/* After the run's stream has synchronised: SCRS_OK, or the device-side
+ * failure a kernel recorded (SCRS_ERR_DEVICE_TIMEOUT). */
+SCRS_API int32_t scrs_stripe_batch_check(scrs_stripe_batch* batch, scrs_error* err);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,107 @@
+"""Batched GF(256) stripes in one persistent launch (include/scrs_gpu.h
+scrs_stripe_batch_*): many independent encode / decode stripes of uneven
+geometry, device-resident buffers, per-stripe decode matrices built on the
+device, optional CUDA-graph replay, and the one-launch-per-stripe baseline."""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+from .api import Engine, Library, _Error, make_error, _stream_ptr
+
+OP_ENCODE = 0
+OP_DECODE = 1
+
+
+class _Desc(C.Structure):
+    _fields_ = [("op", C.c_int32), ("engine", C.c_int32), ("k", C.c_uint32), ("m", C.c_uint32),
+                ("symbol_len", C.c_uint64), ("in_", C.c_void_p), ("out", C.c_void_p),
+                ("indices", C.POINTER(C.c_uint16))]
+
+
+@dataclass
+class Stripe:
+    """One stripe: device pointers (ints) for ``in_ptr`` / ``out_ptr``.
+
+    encode: in = k*L data, out = m*L repairs.
+    decode: in = k received rows (row q is codeword index ``indices[q]``),
+            out = k*L data.
+    """
+
+    op: int
+    engine: Engine
+    k: int
+    m: int
+    symbol_len: int
+    in_ptr: int
+    out_ptr: int
+    indices: Optional[Sequence[int]] = None
+
+
+def _bind(lib: Library):
+    L = lib.lib
+    if getattr(lib, "_batch_bound", False):
+        return
+    L.scrs_stripe_batch_create.restype = C.c_int32
+    L.scrs_stripe_batch_create.argtypes = [C.c_uint64, C.c_uint64, C.POINTER(C.c_void_p), C.POINTER(_Error)]
+    L.scrs_stripe_batch_destroy.restype = None
+    L.scrs_stripe_batch_destroy.argtypes = [C.c_void_p]
+    L.scrs_stripe_batch_set.restype = C.c_int32
+    L.scrs_stripe_batch_set.argtypes = [C.c_void_p, C.POINTER(_Desc), C.c_uint64, C.POINTER(_Error)]
+    L.scrs_stripe_batch_run.restype = C.c_int32
+    L.scrs_stripe_batch_run.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(_Error)]
+    L.scrs_stripe_batch_run_plain.restype = C.c_int32
+    L.scrs_stripe_batch_run_plain.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(_Error)]
+    L.scrs_stripe_batch_last_launches.restype = C.c_uint64
+    L.scrs_stripe_batch_last_launches.argtypes = [C.c_void_p]
+    L.scrs_stripe_batch_check.restype = C.c_int32
+    L.scrs_stripe_batch_check.argtypes = [C.c_void_p, C.POINTER(_Error)]
+    lib._batch_bound = True
+
+
+class StripeBatch:
+    def __init__(self, lib: Library, max_stripes: int, max_items: int = 0):
+        _bind(lib)
+        self._lib = lib
+        self._ptr = C.c_void_p()
+        err = _Error()
+        lib.check(lib.lib.scrs_stripe_batch_create(max_stripes, max_items, C.byref(self._ptr), C.byref(err)), err)
+        self._keep = []
+
+    def __del__(self):
+        if getattr(self, "_ptr", None) is not None and self._ptr.value:
+            self._lib.lib.scrs_stripe_batch_destroy(self._ptr)
+            self._ptr = None
+
+    def set(self, stripes: Sequence[Stripe]):
+        n = len(stripes)
+        arr = (_Desc * max(n, 1))()
+        keep = []
+        for i, s in enumerate(stripes):
+            idx = None
+            if s.indices is not None:
+                idx = (C.c_uint16 * len(s.indices))(*[int(x) for x in s.indices])
+                keep.append(idx)
+            arr[i] = _Desc(int(s.op), int(s.engine), s.k, s.m, s.symbol_len, s.in_ptr, s.out_ptr,
+                           C.cast(idx, C.POINTER(C.c_uint16)) if idx is not None else None)
+        err = _Error()
+        self._lib.check(self._lib.lib.scrs_stripe_batch_set(self._ptr, arr, n, C.byref(err)), err)
+        self._keep = keep
+
+    def run(self, stream=None, graph: bool = False):
+        err = _Error()
+        self._lib.check(self._lib.lib.scrs_stripe_batch_run(self._ptr, _stream_ptr(stream), 1 if graph else 0,
+                                                            C.byref(err)), err)
+
+    def run_plain(self, stream=None):
+        err = _Error()
+        self._lib.check(self._lib.lib.scrs_stripe_batch_run_plain(self._ptr, _stream_ptr(stream), C.byref(err)), err)
+
+    def check(self):
+        err = _Error()
+        self._lib.check(self._lib.lib.scrs_stripe_batch_check(self._ptr, C.byref(err)), err)
+
+    @property
+    def last_launches(self) -> int:
+        return int(self._lib.lib.scrs_stripe_batch_last_launches(self._ptr))

@@ -1,0 +1,60 @@
+"""Build the sm_100a CUDA library in-tree: scrs_b200/_lib/libscrs_b200.so.
+
+    python -m scrs_b200.build
+
+nvcc compiles every translation unit for sm_100a only
+(-gencode arch=compute_100a,code=sm_100a) with the CUDA runtime linked
+statically, so the library shares the driver's primary context with any
+other runtime (torch) in the process.
+"""
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+OUT = HERE / "_lib" / "libscrs_b200.so"
+SOURCES = ["mxk_kernels.cu", "afft.cu", "engines.cu", "batch.cu", "noalloc.cu"]
+FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-gencode", "arch=compute_100a,code=sm_100a",
+         "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
+
+
+def nvcc() -> str:
+    cand = os.environ.get("NVCC") or "/usr/local/cuda/bin/nvcc"
+    return cand if Path(cand).exists() else "nvcc"
+
+
+def build(verbose: bool = False, force: bool = False) -> Path:
+    srcs = [CSRC / s for s in SOURCES if (CSRC / s).exists()]
+    deps = srcs + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [HERE.parent / "include" / "scrs_gpu.h"]
+    if OUT.exists() and not force and all(OUT.stat().st_mtime >= d.stat().st_mtime for d in deps):
+        return OUT
+    obj_dir = HERE / "_lib" / "obj"
+    obj_dir.mkdir(parents=True, exist_ok=True)
+    objs = []
+    procs = []
+    for s in srcs:
+        o = obj_dir / (s.stem + ".o")
+        objs.append(o)
+        cmd = [nvcc(), *FLAGS, "-c", str(s), "-o", str(o)]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    failed = False
+    for cmd, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0 or verbose:
+            sys.stderr.write(out)
+        if p.returncode != 0:
+            failed = True
+    if failed:
+        raise RuntimeError("nvcc compilation failed")
+    link = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "static",
+            *[str(o) for o in objs], "-o", str(OUT)]
+    subprocess.run(link, check=True)
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, force=True))

@@ -1,0 +1,61 @@
+// Additive-FFT engine over GF(2^16) on the device (scrs/src/afft/*.rs).
+//
+// Every systematic encode and erasure decode is the same computation: given
+// the code polynomial F (degree < k, novel basis) at a known point set, with
+// erased set E and locator L(x) = prod_{e in E}(x + e),
+//   F(e) = (F L)'(e) / L'(e)  for e in E
+// (scrs/src/afft/decoder.rs:294-357).  Encode takes E = [k, ts) and reads the
+// repairs at points k..n-1; decode takes E = the untransmitted and lost points
+// and reads the missing data points.  F is unique, so the repairs equal the
+// reference's truncated-transform encode (afft/encoder.rs:150-214) byte for
+// byte.
+#pragma once
+
+#include <stdint.h>
+
+#include <vector>
+
+#include "runtime.h"
+
+namespace scrs {
+
+class AfftWorkspace;
+
+class AfftCodec {
+   public:
+    int32_t init(uint64_t k, uint64_t m, uint64_t L, scrs_error* err);
+    // d_data: k rows; d_repairs: m rows.
+    int32_t encode(const uint8_t* d_data, uint8_t* d_repairs, AfftWorkspace& ws, int32_t* status,
+                   cudaStream_t st, scrs_error* err) const;
+    // d_payloads: n rows in codeword order (only rows with have[i] != 0 are read);
+    // d_out: k rows of data.
+    int32_t decode(const uint8_t* d_payloads, const uint8_t* have, uint8_t* d_out, AfftWorkspace& ws,
+                   int32_t* status, cudaStream_t st, scrs_error* err) const;
+
+    uint64_t k = 0, m = 0, n = 0, L = 0, padded_k = 0, ts = 0;
+    uint32_t log_ts = 0;
+    DevBuf factors;                 // uint16[ts], heap layout (transform.rs:30-61)
+    uint16_t deriv_factors[16] = {};
+    DevBuf enc_values, enc_derivs;  // encode locator for E = [k, ts): uint16[ts]
+};
+
+class AfftWorkspace {
+   public:
+    int32_t init_encode(const AfftCodec& c, scrs_error* err);
+    int32_t init_decode(const AfftCodec& c, scrs_error* err);
+    DevBuf work0, work1;            // ts * L bytes, bit-sliced rows
+    DevBuf known;                   // uint8[ts]
+    DevBuf wht_a, wht_b;            // uint32[ts]
+    DevBuf values, derivs;          // uint16[ts]
+    DevBuf rows;                    // uint16 lists for the output stage
+    std::vector<uint8_t> host_known;
+    std::vector<uint16_t> host_rows;
+    uint64_t k = 0, m = 0, L = 0;
+};
+
+// Locator evaluations for a known-point mask (decoder.rs:672-714), on the
+// device: values[x] = L(x) for known x, derivs[x] = L'(x) for erased x.
+int32_t afft_locator_device(const uint8_t* d_known, uint32_t ts, uint32_t* wa, uint32_t* wb, uint16_t* values,
+                            uint16_t* derivs, cudaStream_t st, scrs_error* err);
+
+}  // namespace scrs

@@ -1,0 +1,286 @@
+// Batched GF(256) stripes: many independent BatchCodec::encode_into
+// (batch/codec.rs:156) and decode_into_with (batch/codec.rs:278) calls of
+// uneven geometry, run as one device work queue.
+//
+//   set():  validate descriptors, build per-stripe tasks and the decode
+//           lists on the host, upload everything in one copy;
+//   run():  one plan launch builds every decode matrix on the device (the
+//           closed-form reduced Cauchy solve), one persistent launch drains
+//           the (stripe, chunk) work queue; optionally replayed as a graph;
+//   run_plain(): the same work as one plan + one multiply-XOR launch per
+//           stripe, the baseline the persistent form is measured against.
+#include <algorithm>
+#include <map>
+#include <memory>
+#include <new>
+#include <tuple>
+
+#include "host_field.h"
+#include "runtime.h"
+
+using namespace scrs;
+
+struct scrs_stripe_batch {
+    uint64_t max_stripes = 0, max_items = 0;
+    StatusWord status;
+    DevBuf d_tasks, d_plans, d_counter, d_arena;
+    std::vector<MxkTask> tasks;
+    std::vector<CauchyPlanTask> plans;
+    std::vector<uint8_t> arena;
+    uint32_t total_items = 0, max_in = 1, max_plan_r = 0;
+    cudaGraphExec_t graph = nullptr;
+    uint64_t graph_launches = 0;  // kernels in the captured graph
+    uint64_t last_launches = 0;
+    int sm_count = 0;
+    ~scrs_stripe_batch() {
+        if (graph) cudaGraphExecDestroy(graph);
+    }
+};
+
+extern "C" int32_t scrs_stripe_batch_create(uint64_t max_stripes, uint64_t max_items, scrs_stripe_batch** out,
+                                            scrs_error* err) {
+    if (!out) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
+    if (max_stripes == 0 || max_stripes > (1u << 24) || max_items > 0xFFFFFFFFull)
+        return set_err(err, SCRS_ERR_BAD_ARGUMENT, 1);
+    std::unique_ptr<scrs_stripe_batch> b(new (std::nothrow) scrs_stripe_batch());
+    if (!b) return set_err(err, SCRS_ERR_OUT_OF_MEMORY, sizeof(scrs_stripe_batch));
+    b->max_stripes = max_stripes;
+    b->max_items = max_items ? max_items : 0xFFFFFFFFull;
+    int dev = 0;
+    SCRS_CUDA(cudaGetDevice(&dev));
+    SCRS_CUDA(cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, dev));
+    SCRS_CUDA(b->status.init());
+    SCRS_CUDA(b->d_tasks.ensure(max_stripes * sizeof(MxkTask)));
+    SCRS_CUDA(b->d_plans.ensure(max_stripes * sizeof(CauchyPlanTask)));
+    SCRS_CUDA(b->d_counter.ensure(64));
+    b->tasks.reserve(max_stripes);
+    b->plans.reserve(max_stripes);
+    *out = b.release();
+    return set_err(err, SCRS_OK);
+}
+
+extern "C" void scrs_stripe_batch_destroy(scrs_stripe_batch* b) { delete b; }
+
+extern "C" uint64_t scrs_stripe_batch_last_launches(const scrs_stripe_batch* b) {
+    return b ? b->last_launches : 0;
+}
+
+extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe_desc* descs, uint64_t count,
+                                         scrs_error* err) {
+    if (!b || (count && !descs)) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
+    if (count > b->max_stripes) return set_err(err, SCRS_ERR_CAPACITY, count, b->max_stripes);
+    // ---- validate and size the arena
+    size_t arena_bytes = 0;
+    std::map<std::tuple<int, uint32_t, uint32_t>, size_t> coef_off;
+    uint64_t items = 0;
+    auto align16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    for (uint64_t s = 0; s < count; s++) {
+        const scrs_stripe_desc& d = descs[s];
+        if (d.op != SCRS_OP_ENCODE && d.op != SCRS_OP_DECODE) return set_err(err, SCRS_ERR_BAD_ARGUMENT, 1, s);
+        if (d.engine != SCRS_ENGINE_STANDARD_CAUCHY && d.engine != SCRS_ENGINE_GOOD_CAUCHY)
+            return set_err(err, SCRS_ERR_BAD_ARGUMENT, 2, s);
+        if (d.k == 0 || d.m == 0) return set_err(err, SCRS_CONFIG_ZERO_DIMENSION, 0, s);
+        if (d.symbol_len == 0) return set_err(err, SCRS_CONFIG_ZERO_SYMBOL_LEN, 0, s);
+        const uint64_t cap = d.engine == SCRS_ENGINE_STANDARD_CAUCHY ? 256 : 255;
+        if ((uint64_t)d.k + d.m > cap) return set_err(err, SCRS_CONFIG_TOO_MANY_SYMBOLS, cap, s);
+        if (!d.in || !d.out) return set_err(err, SCRS_ERR_NULL_ARGUMENT, 0, s);
+        items += n_chunks(d.symbol_len, false);
+        if (d.op == SCRS_OP_ENCODE) {
+            auto key = std::make_tuple(d.engine, d.k, d.m);
+            if (!coef_off.count(key)) {
+                coef_off[key] = arena_bytes;
+                arena_bytes = align16(arena_bytes + (size_t)d.k * d.m);
+            }
+        } else {
+            if (!d.indices) return set_err(err, SCRS_ERR_NULL_ARGUMENT, 0, s);
+            const uint32_t n = d.k + d.m;
+            uint8_t seen[256] = {0};
+            uint32_t r = 0;
+            for (uint32_t q = 0; q < d.k; q++) {
+                uint32_t i = d.indices[q];
+                if (i >= n) return set_err(err, SCRS_DECODE_INDEX_OUT_OF_RANGE, i, n);
+                if (seen[i]) return set_err(err, SCRS_DECODE_DUPLICATE_INDEX, i, s);
+                seen[i] = 1;
+                if (i >= d.k) r++;
+            }
+            // lists: in_rows[k] pass_rows[k] out_rows[r] missing[r] repairs[r] present[k-r]; coef[k*r]
+            arena_bytes = align16(arena_bytes + 2 * ((size_t)3 * d.k + 3 * r));
+            arena_bytes = align16(arena_bytes + (size_t)d.k * std::max<uint32_t>(r, 1));
+        }
+    }
+    if (items > b->max_items || items > 0xFFFFFFFFull) return set_err(err, SCRS_ERR_CAPACITY, items, b->max_items);
+    b->arena.assign(arena_bytes + 16, 0);
+    SCRS_CUDA(b->d_arena.ensure(b->arena.size()));
+    uint8_t* dbase = b->d_arena.as<uint8_t>();
+    for (auto& kv : coef_off)
+        hf::gf8_coefficients(std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first),
+                             b->arena.data() + kv.second);
+    // ---- tasks
+    b->tasks.clear();
+    b->plans.clear();
+    size_t off = 0;
+    for (auto& kv : coef_off) off = std::max(off, align16(kv.second + (size_t)std::get<1>(kv.first) * std::get<2>(kv.first)));
+    uint32_t item = 0, max_in = 1, max_r = 0;
+    for (uint64_t s = 0; s < count; s++) {
+        const scrs_stripe_desc& d = descs[s];
+        MxkTask T{};
+        T.in = d.in;
+        T.out = d.out;
+        T.L = d.symbol_len;
+        T.in_stride = d.symbol_len;
+        T.out_stride = d.symbol_len;
+        T.n_in = d.k;
+        T.n_items = n_chunks(d.symbol_len, false);
+        T.item_begin = item;
+        T.aligned = (d.symbol_len % 16 == 0 && aligned16(d.in) && aligned16(d.out)) ? 1u : 0u;
+        if (d.op == SCRS_OP_ENCODE) {
+            T.coef = dbase + coef_off[std::make_tuple(d.engine, d.k, d.m)];
+            T.n_out = d.m;
+            T.ld = d.m;
+        } else {
+            const uint32_t k = d.k, n = d.k + d.m;
+            std::vector<uint16_t> row_of(n, kNoRow);
+            for (uint32_t q = 0; q < k; q++) row_of[d.indices[q]] = (uint16_t)q;
+            std::vector<uint16_t> missing, present, repairs;
+            for (uint32_t i = 0; i < k; i++) (row_of[i] != kNoRow ? present : missing).push_back((uint16_t)i);
+            for (uint32_t j = 0; j < d.m; j++)
+                if (row_of[k + j] != kNoRow) repairs.push_back((uint16_t)j);
+            const uint32_t r = (uint32_t)missing.size(), p = (uint32_t)present.size();
+            uint16_t* L16 = reinterpret_cast<uint16_t*>(b->arena.data() + off);
+            uint16_t* in_rows = L16;
+            uint16_t* pass_rows = L16 + k;
+            uint16_t* out_rows = L16 + 2 * k;
+            uint16_t* l_missing = out_rows + r;
+            uint16_t* l_repairs = l_missing + r;
+            uint16_t* l_present = l_repairs + r;
+            for (uint32_t t = 0; t < r; t++) in_rows[t] = row_of[k + repairs[t]], pass_rows[t] = kNoRow;
+            for (uint32_t z = 0; z < p; z++) in_rows[r + z] = row_of[present[z]], pass_rows[r + z] = present[z];
+            std::copy(missing.begin(), missing.end(), out_rows);
+            std::copy(missing.begin(), missing.end(), l_missing);
+            std::copy(repairs.begin(), repairs.end(), l_repairs);
+            std::copy(present.begin(), present.end(), l_present);
+            const size_t dl = (size_t)(reinterpret_cast<uint8_t*>(L16) - b->arena.data());
+            uint16_t* dL16 = reinterpret_cast<uint16_t*>(dbase + dl);
+            off = align16(off + 2 * ((size_t)3 * k + 3 * r));
+            uint8_t* dcoef = dbase + off;
+            off = align16(off + (size_t)k * std::max<uint32_t>(r, 1));
+            T.in_rows = dL16;
+            T.pass_rows = dL16 + k;
+            T.out_rows = dL16 + 2 * k;
+            T.coef = dcoef;
+            T.n_out = r;
+            T.ld = std::max<uint32_t>(r, 1);
+            if (r) {
+                CauchyPlanTask P{};
+                P.r = r;
+                P.p = p;
+                P.ld = r;
+                P.engine = (uint32_t)d.engine;
+                P.k = k;
+                P.missing = dL16 + 2 * k + r;
+                P.repairs = dL16 + 2 * k + 2 * r;
+                P.present = dL16 + 2 * k + 3 * r;
+                P.coef = dcoef;
+                b->plans.push_back(P);
+                max_r = std::max(max_r, r);
+            }
+        }
+        max_in = std::max(max_in, T.n_in);
+        item += T.n_items;
+        b->tasks.push_back(T);
+    }
+    b->total_items = item;
+    b->max_in = max_in;
+    b->max_plan_r = max_r;
+    SCRS_CUDA(cudaMemcpy(b->d_arena.p, b->arena.data(), b->arena.size(), cudaMemcpyHostToDevice));
+    if (!b->tasks.empty())
+        SCRS_CUDA(cudaMemcpy(b->d_tasks.p, b->tasks.data(), b->tasks.size() * sizeof(MxkTask), cudaMemcpyHostToDevice));
+    if (!b->plans.empty())
+        SCRS_CUDA(cudaMemcpy(b->d_plans.p, b->plans.data(), b->plans.size() * sizeof(CauchyPlanTask),
+                             cudaMemcpyHostToDevice));
+    if (b->graph) {  // geometry changed: the captured graph no longer applies
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return set_err(err, SCRS_OK);
+}
+
+namespace {
+
+int32_t enqueue_batch(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
+    SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, 4, st));
+    b->last_launches = 0;
+    if (!b->plans.empty()) {
+        SCRS_CUDA(launch_cauchy_plan(b->d_plans.as<CauchyPlanTask>(), (uint32_t)b->plans.size(), 0, b->max_plan_r, st));
+        b->last_launches++;
+    }
+    if (b->total_items) {
+        int grid = b->sm_count * mxk_ctas_per_sm(0, (int)b->max_in);
+        grid = std::min<int>(grid, (int)b->total_items);
+        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), (uint32_t)b->tasks.size(), b->total_items,
+                                   b->d_counter.as<uint32_t>(), b->status.dev, (int)b->max_in, gf256_strategy(), grid,
+                                   st));
+        b->last_launches++;
+    }
+    return SCRS_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t scrs_stripe_batch_run(scrs_stripe_batch* b, void* stream, int32_t use_graph, scrs_error* err) {
+    if (!b) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!use_graph) {
+        int32_t r = enqueue_batch(b, st, err);
+        if (r) return r;
+        return set_err(err, SCRS_OK);
+    }
+    if (!b->graph) {
+        // Capture on a private stream so the legacy default stream can be used by callers.
+        cudaStream_t cap;
+        SCRS_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        int32_t r = SCRS_OK;
+        if (e == cudaSuccess) {
+            r = enqueue_batch(b, cap, err);
+            e = cudaStreamEndCapture(cap, &g);
+        }
+        cudaStreamDestroy(cap);
+        if (r) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        SCRS_CUDA(e);
+        b->graph_launches = b->last_launches;
+        e = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        SCRS_CUDA(e);
+    }
+    SCRS_CUDA(cudaGraphLaunch(b->graph, st));
+    b->last_launches = b->graph_launches;
+    return set_err(err, SCRS_OK);
+}
+
+extern "C" int32_t scrs_stripe_batch_run_plain(scrs_stripe_batch* b, void* stream, scrs_error* err) {
+    if (!b) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
+    cudaStream_t st = (cudaStream_t)stream;
+    b->last_launches = 0;
+    size_t pi = 0;
+    for (const MxkTask& T : b->tasks) {
+        if (T.pass_rows && T.n_out && pi < b->plans.size()) {  // decode stripe with erasures
+            SCRS_CUDA(launch_cauchy_plan_single(b->plans[pi++], 0, st));
+            b->last_launches++;
+        }
+        SCRS_CUDA(launch_mxk_single(T, 0, gf256_strategy(), b->status.dev, 0, st));
+        b->last_launches++;
+    }
+    return set_err(err, SCRS_OK);
+}
+
+extern "C" int32_t scrs_stripe_batch_check(scrs_stripe_batch* b, scrs_error* err) {
+    if (!b) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
+    int32_t r = take_status(b->status, err);
+    if (r) return r;
+    return set_err(err, SCRS_OK);
+}

@@ -1,0 +1,87 @@
+// Device work descriptors and launch entry points shared by the kernels and
+// the host engine code.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace scrs {
+
+constexpr uint16_t kNoRow = 0xFFFFu;
+constexpr int kThreads = 128;   // 4 warps per CTA
+constexpr int kMaxOutGroup = 64; // outputs computed per pass over the inputs
+
+// Field-dependent geometry: bytes a lane owns and the CTA's column chunk.
+template <int kGf16>
+struct FieldGeom {
+    static constexpr int kLaneBytes = kGf16 ? 64 : 32;
+    static constexpr int kChunk = 32 * kLaneBytes;     // bytes per row per CTA
+    static constexpr int kPieces = kLaneBytes / 16;    // 16-byte pieces per lane
+    static constexpr int kSeg = kGf16 ? 16 : 32;       // input rows staged per segment
+    static constexpr int kElem = kGf16 ? 2 : 1;        // coefficient bytes
+};
+
+// One stripe's multiply-XOR job: out_rows[j] = XOR_i coef[i][j] * in_rows[i]
+// for j < n_out, plus verbatim copies in -> pass_rows (decode's present data).
+struct MxkTask {
+    const uint8_t* in;        // row r of the input is in + r * in_stride
+    uint8_t* out;             // row r of the output is out + r * out_stride
+    const void* coef;         // [n_in][ld] elements (uint8 or uint16)
+    const uint16_t* in_rows;  // n_in input row numbers (nullptr: 0..n_in-1)
+    const uint16_t* out_rows; // n_out output row numbers (nullptr: 0..n_out-1)
+    const uint16_t* pass_rows;// n_in output rows for verbatim copies (kNoRow: none)
+    const uint16_t* coef_rows;// n_in coefficient rows (nullptr: input position)
+    uint64_t L;               // bytes per row
+    uint64_t in_stride;
+    uint64_t out_stride;
+    uint32_t n_in;
+    uint32_t n_out;
+    uint32_t ld;
+    uint32_t item_begin;      // first work item (row chunk) of this task
+    uint32_t n_items;         // ceil(L / chunk)
+    uint32_t aligned;         // all rows 16-byte aligned and L % 16 == 0
+    uint32_t accumulate;      // 1: out ^= sum (incremental feed); 0: out = sum
+    uint32_t pad;
+};
+
+// Closed-form reduced Cauchy solve for one decode (decoder/cauchy_inverse.rs:50-167,
+// tower/decoder.rs:433-546).  Rows of `coef`: first the r received repairs
+// (coefficients of the inverse A^-1), then the p present data symbols (the
+// fused coefficients), each row holding r output coefficients.
+struct CauchyPlanTask {
+    uint32_t r;
+    uint32_t p;
+    uint32_t ld;              // row stride of coef, in elements
+    uint32_t engine;          // SCRS_ENGINE_*
+    uint32_t k;
+    uint32_t pad;
+    const uint16_t* missing;  // r data indices
+    const uint16_t* repairs;  // r repair columns j (codeword index k + j)
+    const uint16_t* present;  // p data indices
+    const uint16_t* powers;   // GF(65536): g^i for i < k + m
+    void* coef;
+    uint32_t* work;           // 4*r words of global scratch, or nullptr (shared memory)
+};
+
+// Launchers (return cudaError_t of the launch).
+cudaError_t launch_gf256_mxk(const MxkTask* tasks, uint32_t n_tasks, uint32_t total_items,
+                             uint32_t* work_counter, int32_t* status, int max_in, int strategy,
+                             int grid, cudaStream_t stream);
+cudaError_t launch_gf16_mxk(const MxkTask* tasks, uint32_t n_tasks, uint32_t total_items,
+                            uint32_t* work_counter, int32_t* status, int max_in, int grid,
+                            cudaStream_t stream);
+// One task by value; grid <= 0 means one CTA per row chunk.
+cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int strategy, int32_t* status, int grid,
+                              cudaStream_t stream);
+cudaError_t launch_cauchy_plan_single(const CauchyPlanTask& task, int gf16, cudaStream_t stream);
+// max_smem_r: largest r among tasks whose `work` is nullptr.
+cudaError_t launch_cauchy_plan(const CauchyPlanTask* tasks, uint32_t n_tasks, int gf16, uint32_t max_smem_r,
+                               cudaStream_t stream);
+// Largest r the plan kernel keeps in shared memory.
+constexpr uint32_t kPlanSmemMaxR = 12288;
+// Shared-memory bytes a launch with this many input rows needs.
+size_t mxk_smem_bytes(int gf16, int max_in);
+// CTAs per SM the persistent launch uses for this shared-memory size.
+int mxk_ctas_per_sm(int gf16, int max_in);
+
+}  // namespace scrs

@@ -1,0 +1,311 @@
+"""Parity of the sm_100a engines with the CPU oracle (bit-exact: every output
+is integer/byte work).  Each scenario runs through the C ABI of the CUDA
+library and through the oracle's identical ABI on the same seeded inputs."""
+import numpy as np
+import pytest
+
+from scrs_b200.api import DEPENDENT, DecodeError, EncodeError, Engine, PushOutcome
+
+import gfpy
+from scenarios import (batch_decode, deterministic_subsets, encode_word, k_subsets, lazy_decode,
+                       lcg_permutations)
+
+pytestmark = pytest.mark.gpu
+
+GF256 = [Engine.STANDARD_CAUCHY, Engine.GOOD_CAUCHY]
+
+
+def words_equal(a, b):
+    return all(np.array_equal(x, y) for x, y in zip(a, b))
+
+
+# ---------------------------------------------------------------- GF(256)
+
+@pytest.mark.parametrize("engine", GF256)
+@pytest.mark.parametrize("k,m,L", [(1, 1, 2), (4, 2, 16), (8, 4, 64), (10, 4, 4096), (16, 8, 1024),
+                                   (32, 16, 1024), (64, 16, 4096), (128, 64, 1024), (200, 50, 256),
+                                   (1, 254, 64), (254, 1, 64), (3, 5, 7), (6, 6, 33), (16, 8, 100),
+                                   (10, 4, 1000), (40, 16, 65536), (33, 3, 1025)])
+def test_gf256_encode_matches_oracle(gpu, oracle, engine, k, m, L):
+    if engine == Engine.GOOD_CAUCHY and k + m > 255:
+        pytest.skip("Good Cauchy capacity is 255")
+    p = gpu.resolve(engine, k, m, L)
+    data = gfpy.rng_bytes(k * L, k * 1000 + m)
+    got = np.zeros(m * L, np.uint8)
+    exp = np.zeros(m * L, np.uint8)
+    enc = gpu.batch_encoder(p)
+    s = enc.scratch()
+    enc.encode_into_with(data, got, s)
+    oracle.batch_encoder(p).encode_into(data, exp)
+    assert np.array_equal(got, exp)
+    enc.encode_into_with(data, got, s)  # scratch reuse
+    assert np.array_equal(got, exp)
+
+
+@pytest.mark.parametrize("engine", GF256)
+@pytest.mark.parametrize("k,m,L", [(3, 2, 4), (4, 3, 8), (3, 3, 4), (5, 4, 31)])
+def test_gf256_all_subsets(gpu, oracle, engine, k, m, L):
+    p = gpu.resolve(engine, k, m, L)
+    data = gfpy.rng_bytes(k * L, 99)
+    word = encode_word(gpu, p, data)
+    assert words_equal(word, encode_word(oracle, p, data))
+    for subset in k_subsets(k + m, k):
+        assert np.array_equal(batch_decode(gpu, p, word, subset), data), subset
+        assert np.array_equal(lazy_decode(gpu, p, word, subset[::-1]), data), subset
+
+
+@pytest.mark.parametrize("k,m,L", [(1, 1, 2), (4, 2, 16), (8, 4, 64), (6, 6, 33), (16, 8, 100), (32, 16, 64),
+                                   (10, 4, 4096), (64, 16, 1024), (128, 127, 96)])
+def test_gf256_decode_sampled_patterns(gpu, k, m, L):
+    for engine in GF256:
+        if engine == Engine.GOOD_CAUCHY and k + m > 255:
+            continue
+        p = gpu.resolve(engine, k, m, L)
+        data = gfpy.rng_bytes(k * L, 7 + k)
+        word = encode_word(gpu, p, data)
+        for subset in deterministic_subsets(k, m)[:24]:
+            assert np.array_equal(batch_decode(gpu, p, word, subset), data), subset
+            assert np.array_equal(lazy_decode(gpu, p, word, subset), data), subset
+
+
+def test_gf256_incremental_encoder(gpu, oracle):
+    for k, m, L in [(4, 3, 8), (10, 4, 4096), (60, 16, 33), (100, 100, 2048)]:
+        p = gpu.resolve(Engine.GOOD_CAUCHY, k, m, L)
+        data = gfpy.rng_bytes(k * L, 5 * k)
+        inc, inc_o = gpu.incremental_encoder(p), oracle.incremental_encoder(p)
+        order = list(range(k))[::-1]
+        for t, i in enumerate(order):
+            inc.feed(i, data[i * L:(i + 1) * L])
+            inc_o.feed(i, data[i * L:(i + 1) * L])
+            if t in (0, k // 2):  # partial sums are readable mid-stream
+                assert inc.repair(m - 1) == inc_o.repair(m - 1)
+        assert inc.fed_count() == k
+        assert all(inc.repair(j) == inc_o.repair(j) for j in range(m))
+        with pytest.raises(EncodeError) as e:
+            inc.feed(0, data[:L])
+        assert e.value.variant == "DuplicateData"
+        inc.reset()
+        assert inc.fed_count() == 0 and inc.repair(0) == bytes(L)
+
+
+def error_of(fn):
+    try:
+        fn()
+    except (EncodeError, DecodeError) as e:
+        return e
+    return None
+
+
+def test_gf256_error_parity(gpu, oracle):
+    p = gpu.resolve(Engine.STANDARD_CAUCHY, 3, 2, 4)
+    word = encode_word(oracle, p, np.zeros(12, np.uint8))
+    cases = [
+        [(0, word[0]), (1, word[1])],
+        [(0, word[0]), (1, word[1]), (5, np.zeros(4, np.uint8))],
+        [(0, word[0]), (1, word[1]), (0, word[0])],
+        [(0, word[0]), (1, word[1]), (2, np.zeros(3, np.uint8))],
+    ]
+    for syms in cases:
+        for out_len in (12, 11):
+            eg = error_of(lambda: gpu.batch_decoder(p).decode_into(syms, np.zeros(out_len, np.uint8)))
+            eo = error_of(lambda: oracle.batch_decoder(p).decode_into(syms, np.zeros(out_len, np.uint8)))
+            assert eg == eo and eg is not None
+    enc = gpu.batch_encoder(p)
+    enc_o = oracle.batch_encoder(p)
+    for dl, rl in [(11, 8), (12, 9)]:
+        assert error_of(lambda: enc.encode_into(np.zeros(dl, np.uint8), np.zeros(rl, np.uint8))) == \
+            error_of(lambda: enc_o.encode_into(np.zeros(dl, np.uint8), np.zeros(rl, np.uint8)))
+    other = gpu.batch_decoder(gpu.resolve(Engine.STANDARD_CAUCHY, 4, 2, 4))
+    e = error_of(lambda: gpu.batch_decoder(p).decode_into_with([(0, word[0]), (1, word[1]), (2, word[2])],
+                                                               np.zeros(12, np.uint8), other.scratch()))
+    assert e.variant == "ScratchMismatch"
+
+
+def test_lazy_decoder_push_contract_matches_oracle(gpu, oracle):
+    for engine, k, m, L in [(Engine.GOOD_CAUCHY, 4, 3, 8), (Engine.TOWER, 4, 3, 8), (Engine.AFFT, 4, 3, 8)]:
+        p = gpu.resolve(engine, k, m, L)
+        word = encode_word(oracle, p, gfpy.rng_bytes(k * L, 1))
+        dg, do = gpu.decoder(p), oracle.decoder(p)
+        seq = [k, k, 1, 2, k + 1, 0, 3, 3]
+        for i in seq:
+            rg = error_of(lambda: dg.push(i, word[i])) or dg.received()
+            ro = error_of(lambda: do.push(i, word[i])) or do.received()
+            assert rg == ro
+        assert dg.rank() == do.rank() and dg.is_complete() == do.is_complete()
+        assert dg.finalize() == do.finalize()
+
+
+# ---------------------------------------------------------------- tower
+
+@pytest.mark.parametrize("k,m,L", [(4, 3, 10), (4, 3, 18), (32, 8, 65536), (64, 32, 66), (256, 3, 4),
+                                   (300, 20, 130), (2, 1, 4)])
+def test_tower_encode_matches_oracle(gpu, oracle, k, m, L):
+    p = gpu.resolve(Engine.TOWER, k, m, L)
+    data = gfpy.rng_bytes(k * L, 11 * k + m)
+    assert words_equal(encode_word(gpu, p, data), encode_word(oracle, p, data))
+
+
+def test_tower_recovery(gpu, oracle):
+    k, m, L = 4, 3, 18
+    p = gpu.resolve(Engine.TOWER, k, m, L)
+    data = gfpy.rng_bytes(k * L, 3)
+    word = encode_word(gpu, p, data)
+    for subset in k_subsets(k + m, k):
+        assert np.array_equal(lazy_decode(gpu, p, word, subset), data)
+        assert np.array_equal(batch_decode(gpu, p, word, subset), data)
+    k, m, L = 64, 32, 66
+    p = gpu.resolve(Engine.TOWER, k, m, L)
+    data = gfpy.rng_bytes(k * L, 4)
+    word = encode_word(gpu, p, data)
+    for perm in lcg_permutations(k + m, 8):
+        assert np.array_equal(lazy_decode(gpu, p, word, perm[:k]), data)
+
+
+def test_tower_cfg2_shape(gpu, oracle):
+    """k=32, m=8, L=65536 with 8 data symbols erased (random permutation)."""
+    k, m, L = 32, 8, 65536
+    p = gpu.resolve(Engine.TOWER, k, m, L)
+    data = gfpy.rng_bytes(k * L, 0x5C250002)
+    word = encode_word(gpu, p, data)
+    rng = np.random.default_rng(2)
+    erased = set(rng.choice(k, 8, replace=False).tolist())
+    order = [i for i in rng.permutation(k + m).tolist() if i not in erased][:k]
+    assert np.array_equal(lazy_decode(gpu, p, word, order), data)
+    assert np.array_equal(lazy_decode(oracle, p, word, order), data)
+
+
+# ---------------------------------------------------------------- AFFT
+
+@pytest.mark.parametrize("k,m,L", [(5, 3, 6), (8, 4, 64), (3, 2, 2), (100, 20, 64), (17, 7, 130), (4, 2, 64),
+                                   (16, 4, 40), (256, 64, 48), (512, 128, 40), (1, 1, 2), (8, 8, 4),
+                                   (4096, 4096, 1024)])
+def test_afft_encode_matches_oracle(gpu, oracle, k, m, L):
+    p = gpu.resolve(Engine.AFFT, k, m, L)
+    data = gfpy.rng_bytes(k * L, 17 * k + m)
+    got = np.zeros(m * L, np.uint8)
+    exp = np.zeros(m * L, np.uint8)
+    enc = gpu.batch_encoder(p)
+    enc.encode_into_with(data, got, enc.scratch())
+    oracle.batch_encoder(p).encode_into(data, exp)
+    assert np.array_equal(got, exp)
+
+
+@pytest.mark.parametrize("k,m,L", [(4, 4, 10), (5, 3, 6)])
+def test_afft_exhaustive_recovery(gpu, k, m, L):
+    p = gpu.resolve(Engine.AFFT, k, m, L)
+    data = gfpy.rng_bytes(k * L, 8)
+    word = encode_word(gpu, p, data)
+    for subset in k_subsets(k + m, k):
+        assert np.array_equal(lazy_decode(gpu, p, word, subset), data), subset
+        assert np.array_equal(batch_decode(gpu, p, word, subset), data), subset
+
+
+def test_afft_random_and_large_patterns(gpu, oracle):
+    for k, m, L in [(32, 16, 34), (16, 8, 64), (300, 2, 2)]:
+        p = gpu.resolve(Engine.AFFT, k, m, L)
+        data = gfpy.rng_bytes(k * L, k)
+        word = encode_word(gpu, p, data)
+        for perm in lcg_permutations(k + m, 6):
+            assert np.array_equal(lazy_decode(gpu, p, word, perm[:k]), data)
+    # the config-3a shape: decode from a random half of 8192 points
+    k, m, L = 4096, 4096, 1024
+    p = gpu.resolve(Engine.AFFT, k, m, L)
+    data = gfpy.rng_bytes(k * L, 0x5C250003)
+    word = encode_word(gpu, p, data)
+    sel = np.random.default_rng(3).permutation(k + m)[:k].tolist()
+    assert np.array_equal(lazy_decode(gpu, p, word, sel), data)
+
+
+# ---------------------------------------------------------------- device-pointer forms
+
+def test_device_pointer_entry_points(gpu, oracle):
+    torch = pytest.importorskip("torch")
+    k, m, L = 10, 4, 4096
+    p = gpu.resolve(Engine.GOOD_CAUCHY, k, m, L)
+    data = gfpy.rng_bytes(k * L, 42)
+    exp = np.zeros(m * L, np.uint8)
+    oracle.batch_encoder(p).encode_into(data, exp)
+    d_data = torch.from_numpy(data).cuda()
+    d_rep = torch.zeros(m * L, dtype=torch.uint8, device="cuda")
+    enc = gpu.batch_encoder(p)
+    enc.encode_into_with(d_data, d_rep, enc.scratch())
+    torch.cuda.synchronize()
+    assert np.array_equal(d_rep.cpu().numpy(), exp)
+    word = [data[i * L:(i + 1) * L] for i in range(k)] + [exp[j * L:(j + 1) * L] for j in range(m)]
+    idx = [0, 2, 3, 4, 6, 8, 10, 11, 12, 13]
+    rows = torch.from_numpy(np.concatenate([word[i] for i in idx])).cuda()
+    out = torch.zeros(k * L, dtype=torch.uint8, device="cuda")
+    dec = gpu.batch_decoder(p)
+    dec.decode_into_with((idx, rows), out, dec.scratch())
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), data)
+    # lazy decoder with device pushes and device finalize
+    ld = gpu.decoder(p)
+    for i in idx:
+        ld.push(i, torch.from_numpy(word[i]).cuda())
+    out2 = torch.zeros(k * L, dtype=torch.uint8, device="cuda")
+    ld.finalize_into_with(out2, ld.scratch())
+    torch.cuda.synchronize()
+    assert np.array_equal(out2.cpu().numpy(), data)
+
+
+# ---------------------------------------------------------------- batched stripes
+
+def make_mixed_batch(torch, n_stripes, seed, lens=(1024, 4096, 65536), kmax=64, mmax=16):
+    from scrs_b200.batch import OP_DECODE, OP_ENCODE, Stripe
+
+    rng = np.random.default_rng(seed)
+    specs = []
+    for s in range(n_stripes):
+        k = int(rng.integers(4, kmax + 1))
+        m = int(rng.integers(1, mmax + 1))
+        L = int(rng.choice(lens))
+        engine = Engine.STANDARD_CAUCHY if rng.integers(0, 2) else Engine.GOOD_CAUCHY
+        op = OP_ENCODE if s % 2 == 0 else OP_DECODE
+        specs.append((op, engine, k, m, L))
+    return specs, rng
+
+
+def test_stripe_batch_matches_oracle(gpu, oracle):
+    torch = pytest.importorskip("torch")
+    from scrs_b200.batch import OP_DECODE, OP_ENCODE, Stripe, StripeBatch
+
+    specs, rng = make_mixed_batch(torch, 96, 4, lens=(1024, 4096, 1000, 64))
+    stripes, expect, outs, keep = [], [], [], []
+    for op, engine, k, m, L in specs:
+        p = oracle.resolve(engine, k, m, L)
+        data = rng.integers(0, 256, k * L, dtype=np.uint8)
+        if op == OP_ENCODE:
+            exp = np.zeros(m * L, np.uint8)
+            oracle.batch_encoder(p).encode_into(data, exp)
+            d_in = torch.from_numpy(data).cuda()
+            d_out = torch.zeros(m * L, dtype=torch.uint8, device="cuda")
+            stripes.append(Stripe(op, engine, k, m, L, d_in.data_ptr(), d_out.data_ptr()))
+            expect.append(exp)
+        else:
+            word = encode_word(oracle, p, data)
+            e = int(rng.integers(0, min(k, m) + 1))
+            erased = rng.choice(k, e, replace=False).tolist()
+            repairs = rng.choice(m, e, replace=False).tolist()
+            idx = [i for i in range(k) if i not in erased] + [k + j for j in repairs]
+            idx = rng.permutation(idx).tolist()
+            d_in = torch.from_numpy(np.concatenate([word[i] for i in idx])).cuda()
+            d_out = torch.zeros(k * L, dtype=torch.uint8, device="cuda")
+            stripes.append(Stripe(op, engine, k, m, L, d_in.data_ptr(), d_out.data_ptr(), idx))
+            expect.append(data)
+        keep.append(d_in)
+        outs.append(d_out)
+    b = StripeBatch(gpu.lib, len(stripes))
+    b.set(stripes)
+    for mode in ("persistent", "graph", "plain", "graph"):
+        for o in outs:
+            o.zero_()
+        if mode == "plain":
+            b.run_plain()
+        else:
+            b.run(graph=(mode == "graph"))
+        torch.cuda.synchronize()
+        b.check()
+        for o, exp in zip(outs, expect):
+            assert np.array_equal(o.cpu().numpy(), exp), mode
+    assert b.last_launches == 2  # plan + persistent drain
