@@ -69,8 +69,8 @@ extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe
                                          scrs_error* err) {
     if (!b || (count && !descs)) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
     if (count > b->max_stripes) return set_err(err, SCRS_ERR_CAPACITY, count, b->max_stripes);
-    // ---- validate and size the arena
-    size_t arena_bytes = 0;
+    // ---- validate and size the arena: [encode coefficient tables][decode slots]
+    size_t coef_bytes = 0, slot_bytes = 0;
     std::map<std::tuple<int, uint32_t, uint32_t>, size_t> coef_off;
     uint64_t items = 0;
     auto align16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
@@ -88,8 +88,8 @@ extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe
         if (d.op == SCRS_OP_ENCODE) {
             auto key = std::make_tuple(d.engine, d.k, d.m);
             if (!coef_off.count(key)) {
-                coef_off[key] = arena_bytes;
-                arena_bytes = align16(arena_bytes + (size_t)d.k * d.m);
+                coef_off[key] = coef_bytes;
+                coef_bytes = align16(coef_bytes + (size_t)d.k * d.m);
             }
         } else {
             if (!d.indices) return set_err(err, SCRS_ERR_NULL_ARGUMENT, 0, s);
@@ -104,11 +104,12 @@ extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe
                 if (i >= d.k) r++;
             }
             // lists: in_rows[k] pass_rows[k] out_rows[r] missing[r] repairs[r] present[k-r]; coef[k*r]
-            arena_bytes = align16(arena_bytes + 2 * ((size_t)3 * d.k + 3 * r));
-            arena_bytes = align16(arena_bytes + (size_t)d.k * std::max<uint32_t>(r, 1));
+            slot_bytes = align16(slot_bytes + 2 * ((size_t)3 * d.k + 3 * r));
+            slot_bytes = align16(slot_bytes + (size_t)d.k * std::max<uint32_t>(r, 1));
         }
     }
     if (items > b->max_items || items > 0xFFFFFFFFull) return set_err(err, SCRS_ERR_CAPACITY, items, b->max_items);
+    const size_t arena_bytes = coef_bytes + slot_bytes;
     b->arena.assign(arena_bytes + 16, 0);
     SCRS_CUDA(b->d_arena.ensure(b->arena.size()));
     uint8_t* dbase = b->d_arena.as<uint8_t>();
@@ -118,8 +119,7 @@ extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe
     // ---- tasks
     b->tasks.clear();
     b->plans.clear();
-    size_t off = 0;
-    for (auto& kv : coef_off) off = std::max(off, align16(kv.second + (size_t)std::get<1>(kv.first) * std::get<2>(kv.first)));
+    size_t off = coef_bytes;  // decode slots follow the coefficient tables
     uint32_t item = 0, max_in = 1, max_r = 0;
     for (uint64_t s = 0; s < count; s++) {
         const scrs_stripe_desc& d = descs[s];
@@ -192,6 +192,7 @@ extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe
     b->total_items = item;
     b->max_in = max_in;
     b->max_plan_r = max_r;
+    if (off > arena_bytes) return set_err(err, SCRS_ERR_CAPACITY, off, arena_bytes);  // layout invariant
     SCRS_CUDA(cudaMemcpy(b->d_arena.p, b->arena.data(), b->arena.size(), cudaMemcpyHostToDevice));
     if (!b->tasks.empty())
         SCRS_CUDA(cudaMemcpy(b->d_tasks.p, b->tasks.data(), b->tasks.size() * sizeof(MxkTask), cudaMemcpyHostToDevice));
