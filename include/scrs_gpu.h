@@ -317,6 +317,12 @@ SCRS_API int32_t scrs_stripe_batch_run_plain(scrs_stripe_batch* batch, void* str
                                     scrs_error* err);
 /* Number of kernels the last run launched (for launch accounting). */
 SCRS_API uint64_t scrs_stripe_batch_last_launches(const scrs_stripe_batch* batch);
+/* Measurement form of scrs_stripe_batch_run (no graph): brackets the plan
+ * launch and the persistent drain launch with CUDA events on `stream`,
+ * synchronises, and reports each launch's device time in milliseconds. */
+SCRS_API int32_t scrs_stripe_batch_run_timed(scrs_stripe_batch* batch, void* stream,
+                                             float* plan_ms, float* drain_ms,
+                                             scrs_error* err);
 /* After the run's stream has synchronised: SCRS_OK, or the device-side
  * failure a kernel recorded (SCRS_ERR_DEVICE_TIMEOUT). */
 SCRS_API int32_t scrs_stripe_batch_check(scrs_stripe_batch* batch, scrs_error* err);

@@ -20,6 +20,14 @@ class _Desc(C.Structure):
                 ("indices", C.POINTER(C.c_uint16))]
 
 
+import numpy as _np
+
+DESC_DTYPE = _np.dtype({"names": ["op", "engine", "k", "m", "symbol_len", "in_", "out", "indices"],
+                        "formats": [_np.int32, _np.int32, _np.uint32, _np.uint32, _np.uint64, _np.uint64,
+                                    _np.uint64, _np.uint64],
+                        "offsets": [0, 4, 8, 12, 16, 24, 32, 40], "itemsize": 48})
+
+
 @dataclass
 class Stripe:
     """One stripe: device pointers (ints) for ``in_ptr`` / ``out_ptr``.
@@ -55,6 +63,9 @@ def _bind(lib: Library):
     L.scrs_stripe_batch_run_plain.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(_Error)]
     L.scrs_stripe_batch_last_launches.restype = C.c_uint64
     L.scrs_stripe_batch_last_launches.argtypes = [C.c_void_p]
+    L.scrs_stripe_batch_run_timed.restype = C.c_int32
+    L.scrs_stripe_batch_run_timed.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                              C.POINTER(_Error)]
     L.scrs_stripe_batch_check.restype = C.c_int32
     L.scrs_stripe_batch_check.argtypes = [C.c_void_p, C.POINTER(_Error)]
     lib._batch_bound = True
@@ -93,6 +104,35 @@ class StripeBatch:
         err = _Error()
         self._lib.check(self._lib.lib.scrs_stripe_batch_run(self._ptr, _stream_ptr(stream), 1 if graph else 0,
                                                             C.byref(err)), err)
+
+    def set_arrays(self, op, engine, k, m, symbol_len, in_ptr, out_ptr, indices=None, k_max=None):
+        """Bulk form of set(): numpy arrays with one entry per stripe.  For
+        decode stripes, ``indices`` is a uint16 array of shape (count, k_max)
+        whose row s holds that stripe's k received codeword indices."""
+        import numpy as np
+
+        n = len(op)
+        desc = np.zeros(n, dtype=DESC_DTYPE)
+        desc["op"], desc["engine"], desc["k"], desc["m"] = op, engine, k, m
+        desc["symbol_len"], desc["in_"], desc["out"] = symbol_len, in_ptr, out_ptr
+        keep = [desc]
+        if indices is not None:
+            idx = np.ascontiguousarray(indices, dtype=np.uint16)
+            keep.append(idx)
+            row_bytes = idx.shape[1] * 2
+            dec = np.asarray(op) == OP_DECODE
+            desc["indices"] = np.where(dec, idx.ctypes.data + np.arange(n, dtype=np.uint64) * row_bytes, 0)
+        err = _Error()
+        ptr = C.cast(desc.ctypes.data, C.POINTER(_Desc))
+        self._lib.check(self._lib.lib.scrs_stripe_batch_set(self._ptr, ptr, n, C.byref(err)), err)
+        self._keep = keep
+
+    def run_timed(self, stream=None):
+        """(plan_ms, drain_ms) of one non-graph run, bracketed by CUDA events."""
+        err, a, b = _Error(), C.c_float(), C.c_float()
+        self._lib.check(self._lib.lib.scrs_stripe_batch_run_timed(self._ptr, _stream_ptr(stream), C.byref(a),
+                                                                  C.byref(b), C.byref(err)), err)
+        return a.value, b.value
 
     def run_plain(self, stream=None):
         err = _Error()

@@ -279,6 +279,38 @@ extern "C" int32_t scrs_stripe_batch_run_plain(scrs_stripe_batch* b, void* strea
     return set_err(err, SCRS_OK);
 }
 
+extern "C" int32_t scrs_stripe_batch_run_timed(scrs_stripe_batch* b, void* stream, float* plan_ms,
+                                               float* drain_ms, scrs_error* err) {
+    if (!b) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaEvent_t ev[3];
+    for (auto& e : ev) SCRS_CUDA(cudaEventCreate(&e));
+    SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, 4, st));
+    b->last_launches = 0;
+    cudaEventRecord(ev[0], st);
+    if (!b->plans.empty()) {
+        SCRS_CUDA(launch_cauchy_plan(b->d_plans.as<CauchyPlanTask>(), (uint32_t)b->plans.size(), 0, b->max_plan_r, st));
+        b->last_launches++;
+    }
+    cudaEventRecord(ev[1], st);
+    if (b->total_items) {
+        int grid = std::min<int>(b->sm_count * mxk_ctas_per_sm(0, (int)b->max_in), (int)b->total_items);
+        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), (uint32_t)b->tasks.size(), b->total_items,
+                                   b->d_counter.as<uint32_t>(), b->status.dev, (int)b->max_in, gf256_strategy(), grid,
+                                   st));
+        b->last_launches++;
+    }
+    cudaEventRecord(ev[2], st);
+    SCRS_CUDA(cudaEventSynchronize(ev[2]));
+    float a = 0, c = 0;
+    cudaEventElapsedTime(&a, ev[0], ev[1]);
+    cudaEventElapsedTime(&c, ev[1], ev[2]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (plan_ms) *plan_ms = a;
+    if (drain_ms) *drain_ms = c;
+    return set_err(err, SCRS_OK);
+}
+
 extern "C" int32_t scrs_stripe_batch_check(scrs_stripe_batch* b, scrs_error* err) {
     if (!b) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
     int32_t r = take_status(b->status, err);
