@@ -306,6 +306,14 @@ SCRS_API void scrs_stripe_batch_destroy(scrs_stripe_batch* batch);
 SCRS_API int32_t scrs_stripe_batch_set(scrs_stripe_batch* batch,
                               const scrs_stripe_desc* descs, uint64_t count,
                               scrs_error* err);
+/* Host-buffer form of scrs_stripe_batch_set: every `in` / `out` pointer is
+ * HOST memory (pinned memory gives asynchronous copies).  The batch owns
+ * device staging sized at this call; each run then copies inputs in,
+ * runs the work and copies outputs back on the run's stream, merging
+ * copies of stripes that are contiguous in host memory. */
+SCRS_API int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* batch,
+                                            const scrs_stripe_desc* descs,
+                                            uint64_t count, scrs_error* err);
 /* Run the uploaded stripes on `stream`: one device-side plan kernel builds
  * every decode matrix, one persistent kernel drains the work queue.  With
  * use_graph != 0 the pair is captured once into a CUDA graph and replayed. */

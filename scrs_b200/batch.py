@@ -57,6 +57,8 @@ def _bind(lib: Library):
     L.scrs_stripe_batch_destroy.argtypes = [C.c_void_p]
     L.scrs_stripe_batch_set.restype = C.c_int32
     L.scrs_stripe_batch_set.argtypes = [C.c_void_p, C.POINTER(_Desc), C.c_uint64, C.POINTER(_Error)]
+    L.scrs_stripe_batch_set_host.restype = C.c_int32
+    L.scrs_stripe_batch_set_host.argtypes = [C.c_void_p, C.POINTER(_Desc), C.c_uint64, C.POINTER(_Error)]
     L.scrs_stripe_batch_run.restype = C.c_int32
     L.scrs_stripe_batch_run.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(_Error)]
     L.scrs_stripe_batch_run_plain.restype = C.c_int32
@@ -105,7 +107,7 @@ class StripeBatch:
         self._lib.check(self._lib.lib.scrs_stripe_batch_run(self._ptr, _stream_ptr(stream), 1 if graph else 0,
                                                             C.byref(err)), err)
 
-    def set_arrays(self, op, engine, k, m, symbol_len, in_ptr, out_ptr, indices=None, k_max=None):
+    def set_arrays(self, op, engine, k, m, symbol_len, in_ptr, out_ptr, indices=None, host=False):
         """Bulk form of set(): numpy arrays with one entry per stripe.  For
         decode stripes, ``indices`` is a uint16 array of shape (count, k_max)
         whose row s holds that stripe's k received codeword indices."""
@@ -124,7 +126,8 @@ class StripeBatch:
             desc["indices"] = np.where(dec, idx.ctypes.data + np.arange(n, dtype=np.uint64) * row_bytes, 0)
         err = _Error()
         ptr = C.cast(desc.ctypes.data, C.POINTER(_Desc))
-        self._lib.check(self._lib.lib.scrs_stripe_batch_set(self._ptr, ptr, n, C.byref(err)), err)
+        fn = self._lib.lib.scrs_stripe_batch_set_host if host else self._lib.lib.scrs_stripe_batch_set
+        self._lib.check(fn(self._ptr, ptr, n, C.byref(err)), err)
         self._keep = keep
 
     def run_timed(self, stream=None):

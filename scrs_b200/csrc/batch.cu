@@ -32,6 +32,15 @@ struct scrs_stripe_batch {
     uint64_t graph_launches = 0;  // kernels in the captured graph
     uint64_t last_launches = 0;
     int sm_count = 0;
+    // host-buffer mode
+    struct Copy {
+        const void* src;
+        void* dst;
+        size_t bytes;
+    };
+    bool host_mode = false;
+    DevBuf stage_in, stage_out;
+    std::vector<Copy> h2d, d2h;
     ~scrs_stripe_batch() {
         if (graph) cudaGraphExecDestroy(graph);
     }
@@ -199,6 +208,7 @@ extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe
     if (!b->plans.empty())
         SCRS_CUDA(cudaMemcpy(b->d_plans.p, b->plans.data(), b->plans.size() * sizeof(CauchyPlanTask),
                              cudaMemcpyHostToDevice));
+    b->host_mode = false;  // scrs_stripe_batch_set_host re-enables it after this call
     if (b->graph) {  // geometry changed: the captured graph no longer applies
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
@@ -206,7 +216,65 @@ extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe
     return set_err(err, SCRS_OK);
 }
 
+extern "C" int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* b, const scrs_stripe_desc* descs,
+                                              uint64_t count, scrs_error* err) {
+    if (!b || (count && !descs)) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
+    if (count > b->max_stripes) return set_err(err, SCRS_ERR_CAPACITY, count, b->max_stripes);
+    size_t in_bytes = 0, out_bytes = 0;
+    for (uint64_t s = 0; s < count; s++) {
+        const scrs_stripe_desc& d = descs[s];
+        const uint64_t rows_out = d.op == SCRS_OP_ENCODE ? d.m : d.k;
+        in_bytes += (((uint64_t)d.k * d.symbol_len) + 15) & ~15ull;
+        out_bytes += ((rows_out * d.symbol_len) + 15) & ~15ull;
+    }
+    SCRS_CUDA(b->stage_in.ensure(in_bytes));
+    SCRS_CUDA(b->stage_out.ensure(out_bytes));
+    std::vector<scrs_stripe_desc> dev(descs, descs + count);
+    b->h2d.clear();
+    b->d2h.clear();
+    size_t oi = 0, oo = 0;
+    for (uint64_t s = 0; s < count; s++) {
+        const scrs_stripe_desc& d = descs[s];
+        if (!d.in || !d.out) return set_err(err, SCRS_ERR_NULL_ARGUMENT, 0, s);
+        const uint64_t rows_out = d.op == SCRS_OP_ENCODE ? d.m : d.k;
+        const size_t ib = (size_t)d.k * d.symbol_len, ob = (size_t)rows_out * d.symbol_len;
+        uint8_t* din = b->stage_in.as<uint8_t>() + oi;
+        uint8_t* dout = b->stage_out.as<uint8_t>() + oo;
+        dev[s].in = din;
+        dev[s].out = dout;
+        // merge with the previous copy when both sides are contiguous
+        if (!b->h2d.empty() && (const uint8_t*)b->h2d.back().src + b->h2d.back().bytes == d.in &&
+            (uint8_t*)b->h2d.back().dst + b->h2d.back().bytes == din)
+            b->h2d.back().bytes += ib;
+        else
+            b->h2d.push_back({d.in, din, ib});
+        if (!b->d2h.empty() && (const uint8_t*)b->d2h.back().src + b->d2h.back().bytes == dout &&
+            (uint8_t*)b->d2h.back().dst + b->d2h.back().bytes == d.out)
+            b->d2h.back().bytes += ob;
+        else
+            b->d2h.push_back({dout, d.out, ob});
+        oi += (ib + 15) & ~(size_t)15;
+        oo += (ob + 15) & ~(size_t)15;
+    }
+    int32_t r = scrs_stripe_batch_set(b, dev.data(), count, err);
+    if (r) return r;
+    b->host_mode = true;
+    return set_err(err, SCRS_OK);
+}
+
 namespace {
+
+int32_t copy_in(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
+    if (!b->host_mode) return SCRS_OK;
+    for (auto& c : b->h2d) SCRS_CUDA(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, st));
+    return SCRS_OK;
+}
+
+int32_t copy_out(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
+    if (!b->host_mode) return SCRS_OK;
+    for (auto& c : b->d2h) SCRS_CUDA(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, st));
+    return SCRS_OK;
+}
 
 int32_t enqueue_batch(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
     SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, 4, st));
@@ -231,8 +299,12 @@ int32_t enqueue_batch(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
 extern "C" int32_t scrs_stripe_batch_run(scrs_stripe_batch* b, void* stream, int32_t use_graph, scrs_error* err) {
     if (!b) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
     cudaStream_t st = (cudaStream_t)stream;
+    int32_t r0 = copy_in(b, st, err);
+    if (r0) return r0;
     if (!use_graph) {
         int32_t r = enqueue_batch(b, st, err);
+        if (r) return r;
+        r = copy_out(b, st, err);
         if (r) return r;
         return set_err(err, SCRS_OK);
     }
@@ -260,12 +332,16 @@ extern "C" int32_t scrs_stripe_batch_run(scrs_stripe_batch* b, void* stream, int
     }
     SCRS_CUDA(cudaGraphLaunch(b->graph, st));
     b->last_launches = b->graph_launches;
+    r0 = copy_out(b, st, err);
+    if (r0) return r0;
     return set_err(err, SCRS_OK);
 }
 
 extern "C" int32_t scrs_stripe_batch_run_plain(scrs_stripe_batch* b, void* stream, scrs_error* err) {
     if (!b) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
     cudaStream_t st = (cudaStream_t)stream;
+    int32_t r0 = copy_in(b, st, err);
+    if (r0) return r0;
     b->last_launches = 0;
     size_t pi = 0;
     for (const MxkTask& T : b->tasks) {
@@ -276,6 +352,8 @@ extern "C" int32_t scrs_stripe_batch_run_plain(scrs_stripe_batch* b, void* strea
         SCRS_CUDA(launch_mxk_single(T, 0, gf256_strategy(), b->status.dev, 0, st));
         b->last_launches++;
     }
+    r0 = copy_out(b, st, err);
+    if (r0) return r0;
     return set_err(err, SCRS_OK);
 }
 
