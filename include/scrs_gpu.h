@@ -209,6 +209,25 @@ SCRS_API int32_t scrs_batch_decode_into_with_device(scrs_batch_decoder* dec,
                                            scrs_batch_decode_scratch* scratch,
                                            void* stream, scrs_error* err);
 
+/* GF(256) batch decode that allocates nothing (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc: the allocation may
+ * synchronise the device, which a latency-bound receive loop cannot afford,
+ * and a process that reserved its device memory at start-up has no headroom
+ * for per-codec buffers.  Same inputs, outputs and validation as
+ * scrs_batch_decode_into_with_device, without a decoder handle or scratch:
+ * the reconstruction recipe lives in one fixed 16 KiB device array built into
+ * the library.  Decodes whose recipe exceeds it (2*(3k+3r) + k*r bytes for
+ * r erased data symbols) fail with SCRS_ERR_CAPACITY (a = needed, b = 16384).
+ * Calls share that array: calls whose device work overlaps race and must be
+ * ordered on one stream.  The first call on a device looks up the array's
+ * address; make it before any stream capture on that device. */
+SCRS_API int32_t scrs_gf256_decode_static(int32_t engine, uint64_t k,
+                                          uint64_t m, uint64_t symbol_len,
+                                          const uint64_t* indices,
+                                          const uint8_t* d_rows, uint64_t count,
+                                          uint8_t* d_out, uint64_t out_len,
+                                          void* stream, scrs_error* err);
+
 /* ---- IncrementalEncoder: selector.rs:370-429, codec.rs:122-131 ---------- */
 /* UnsupportedMode for Standard Cauchy and AFFT (selector.rs:379). */
 SCRS_API int32_t scrs_incremental_encoder_create(const scrs_profile* profile,
