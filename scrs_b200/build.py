@@ -25,7 +25,15 @@ def nvcc() -> str:
     return cand if Path(cand).exists() else "nvcc"
 
 
+def generate():
+    """Regenerate the PTX jump tables when their generator is newer."""
+    gen, out = CSRC / "gen_brx.py", CSRC / "brx_dispatch.cuh"
+    if not out.exists() or out.stat().st_mtime < gen.stat().st_mtime:
+        subprocess.run([sys.executable, str(gen)], check=True)
+
+
 def build(verbose: bool = False, force: bool = False) -> Path:
+    generate()
     srcs = [CSRC / s for s in SOURCES if (CSRC / s).exists()]
     deps = srcs + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [HERE.parent / "include" / "scrs_gpu.h"]
     if OUT.exists() and not force and all(OUT.stat().st_mtime >= d.stat().st_mtime for d in deps):

@@ -212,7 +212,7 @@ __device__ __forceinline__ void store_planes(uint8_t* p, const uint32_t (&w)[16]
 // (the product evaluations of F*L, decoder.rs:320-333).
 __global__ void __launch_bounds__(128) scale_in_kernel(const uint8_t* payloads, uint64_t L, uint32_t G,
                                                        const uint8_t* known, const uint16_t* values,
-                                                       uint32_t ts, uint8_t* work) {
+                                                       uint32_t ts, uint8_t* work, const uint16_t* row_map) {
     const uint64_t total = (uint64_t)ts * G;
     for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < total;
          x += (uint64_t)gridDim.x * blockDim.x) {
@@ -222,9 +222,10 @@ __global__ void __launch_bounds__(128) scale_in_kernel(const uint8_t* payloads, 
         for (int t = 0; t < 16; t++) acc[t] = 0;
         if (known[row]) {
             uint32_t w[16];
-            load_group_bytes(payloads + (uint64_t)row * L, g, L, w);
+            const uint64_t src = row_map ? row_map[row] : row;
+            load_group_bytes(payloads + src * L, g, L, w);
             bitslice16(w);
-            mul16(values[row], acc, w);
+            mul16<false>(values[row], acc, w);
         }
         store_planes(work + ((uint64_t)row * G + g) * 64, acc);
     }
@@ -249,7 +250,7 @@ __global__ void __launch_bounds__(128) derivative_kernel(const uint8_t* in, uint
             if ((j >> b) & 1u) continue;
             uint32_t w[16];
             load_planes(in + ((uint64_t)(j | (1u << b)) * G + g) * 64, w);
-            mul16(df.f[b], acc, w);
+            mul16<true>(df.f[b], acc, w);
         }
         store_planes(out + ((uint64_t)j * G + g) * 64, acc);
     }
@@ -272,19 +273,20 @@ __global__ void __launch_bounds__(128) scale_out_kernel(const uint8_t* work, uin
         load_planes(work + ((uint64_t)src * G + g) * 64, w);
 #pragma unroll
         for (int q = 0; q < 16; q++) acc[q] = 0;
-        mul16(f, acc, w);
+        mul16<false>(f, acc, w);
         bitslice16(acc);
         store_group_bytes(out + (uint64_t)rows_dst[t] * L, g, L, acc);
     }
 }
 
 __global__ void copy_rows_kernel(const uint8_t* src, uint8_t* dst, uint64_t L, const uint16_t* rows,
-                                 uint32_t count) {
+                                 uint32_t count, const uint16_t* row_map) {
     const uint64_t total = (uint64_t)count * L;
     for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < total;
          x += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t r = rows[x / L];
-        dst[r * L + x % L] = src[r * L + x % L];
+        const uint64_t s = row_map ? row_map[r] : r;
+        dst[r * L + x % L] = src[s * L + x % L];
     }
 }
 
@@ -338,13 +340,13 @@ __global__ void __launch_bounds__(kPassThreads) afft_pass_kernel(uint8_t* work, 
                 wh[4 * q] = h.x, wh[4 * q + 1] = h.y, wh[4 * q + 2] = h.z, wh[4 * q + 3] = h.w;
             }
             if (forward) {  // low ^= f*high; high ^= low
-                if (f) mul16(f, wl, wh);
+                if (f) mul16<false>(f, wl, wh);
 #pragma unroll
                 for (int q = 0; q < 16; q++) wh[q] ^= wl[q];
             } else {  // high ^= low; low ^= f*high
 #pragma unroll
                 for (int q = 0; q < 16; q++) wh[q] ^= wl[q];
-                if (f) mul16(f, wl, wh);
+                if (f) mul16<false>(f, wl, wh);
             }
 #pragma unroll
             for (int q = 0; q < 4; q++) {
@@ -515,6 +517,7 @@ int32_t AfftWorkspace::init_decode(const AfftCodec& c, scrs_error* err) {
     SCRS_CUDA(wht_b.ensure(c.ts * 4));
     SCRS_CUDA(values.ensure(c.ts * 2));
     SCRS_CUDA(derivs.ensure(c.ts * 2));
+    SCRS_CUDA(row_map.ensure(c.n * 2));
     host_known.assign(c.ts, 0);
     host_rows.assign(2 * c.k + 8, 0);
     SCRS_CUDA(rows.ensure(host_rows.size() * 2));
@@ -529,7 +532,7 @@ int32_t AfftCodec::encode(const uint8_t* d_data, uint8_t* d_repairs, AfftWorkspa
     SCRS_CUDA(log16_tables(&lg, &ex));
     scale_in_kernel<<<grid_for(ts * G, 128), 128, 0, st>>>(d_data, L, G, ws.known.as<uint8_t>(),
                                                            enc_values.as<uint16_t>(), (uint32_t)ts,
-                                                           ws.work0.as<uint8_t>());
+                                                           ws.work0.as<uint8_t>(), nullptr);
     SCRS_CUDA(cudaGetLastError());
     SCRS_CUDA(run_transform(ws.work0.as<uint8_t>(), G, (int)log_ts, factors.as<uint16_t>(), false, st));
     DerivFactors df{};
@@ -546,7 +549,7 @@ int32_t AfftCodec::encode(const uint8_t* d_data, uint8_t* d_repairs, AfftWorkspa
 }
 
 int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_t* d_out, AfftWorkspace& ws,
-                          int32_t* status, cudaStream_t st, scrs_error* err) const {
+                          int32_t* status, cudaStream_t st, scrs_error* err, const uint16_t* row_map) const {
     (void)status;
     const uint32_t G = (uint32_t)((L + 63) / 64);
     const uint16_t *lg, *ex;
@@ -564,8 +567,13 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
     SCRS_CUDA(cudaMemcpyAsync(ws.rows.p, ws.host_rows.data(), ws.host_rows.size() * 2, cudaMemcpyHostToDevice, st));
     const uint16_t* d_miss = ws.rows.as<uint16_t>();
     const uint16_t* d_pres = ws.rows.as<uint16_t>() + k;
+    const uint16_t* d_map = nullptr;
+    if (row_map) {
+        SCRS_CUDA(cudaMemcpyAsync(ws.row_map.p, row_map, n * 2, cudaMemcpyHostToDevice, st));
+        d_map = ws.row_map.as<uint16_t>();
+    }
     if (np) {
-        copy_rows_kernel<<<grid_for((uint64_t)np * L, 256), 256, 0, st>>>(d_payloads, d_out, L, d_pres, np);
+        copy_rows_kernel<<<grid_for((uint64_t)np * L, 256), 256, 0, st>>>(d_payloads, d_out, L, d_pres, np, d_map);
         SCRS_CUDA(cudaGetLastError());
     }
     if (nm == 0) return SCRS_OK;
@@ -577,7 +585,7 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
     if (r) return r;
     scale_in_kernel<<<grid_for(ts * G, 128), 128, 0, st>>>(d_payloads, L, G, ws.known.as<uint8_t>(),
                                                            ws.values.as<uint16_t>(), (uint32_t)ts,
-                                                           ws.work0.as<uint8_t>());
+                                                           ws.work0.as<uint8_t>(), d_map);
     SCRS_CUDA(cudaGetLastError());
     SCRS_CUDA(run_transform(ws.work0.as<uint8_t>(), G, (int)log_ts, factors.as<uint16_t>(), false, st));
     DerivFactors df{};

@@ -27,10 +27,11 @@ class AfftCodec {
     // d_data: k rows; d_repairs: m rows.
     int32_t encode(const uint8_t* d_data, uint8_t* d_repairs, AfftWorkspace& ws, int32_t* status,
                    cudaStream_t st, scrs_error* err) const;
-    // d_payloads: n rows in codeword order (only rows with have[i] != 0 are read);
-    // d_out: k rows of data.
+    // d_payloads: rows of received symbols; row of codeword index i is
+    // row_map[i] (host array of n entries) or i when row_map is nullptr.  Only
+    // rows with have[i] != 0 are read.  d_out: k rows of data.
     int32_t decode(const uint8_t* d_payloads, const uint8_t* have, uint8_t* d_out, AfftWorkspace& ws,
-                   int32_t* status, cudaStream_t st, scrs_error* err) const;
+                   int32_t* status, cudaStream_t st, scrs_error* err, const uint16_t* row_map = nullptr) const;
 
     uint64_t k = 0, m = 0, n = 0, L = 0, padded_k = 0, ts = 0;
     uint32_t log_ts = 0;
@@ -48,6 +49,7 @@ class AfftWorkspace {
     DevBuf wht_a, wht_b;            // uint32[ts]
     DevBuf values, derivs;          // uint16[ts]
     DevBuf rows;                    // uint16 lists for the output stage
+    DevBuf row_map;                 // uint16[n] codeword index -> payload row
     std::vector<uint8_t> host_known;
     std::vector<uint16_t> host_rows;
     uint64_t k = 0, m = 0, L = 0;

@@ -23,7 +23,8 @@ using namespace scrs;
 struct scrs_stripe_batch {
     uint64_t max_stripes = 0, max_items = 0;
     StatusWord status;
-    DevBuf d_tasks, d_plans, d_counter, d_arena;
+    DevBuf d_tasks, d_plans, d_counter, d_arena, d_item_task;
+    std::vector<uint32_t> item_task;
     std::vector<MxkTask> tasks;
     std::vector<CauchyPlanTask> plans;
     std::vector<uint8_t> arena;
@@ -200,6 +201,13 @@ extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe
     }
     b->total_items = item;
     b->max_in = max_in;
+    b->item_task.resize(item);
+    for (size_t t = 0; t < b->tasks.size(); t++)
+        std::fill(b->item_task.begin() + b->tasks[t].item_begin,
+                  b->item_task.begin() + b->tasks[t].item_begin + b->tasks[t].n_items, (uint32_t)t);
+    SCRS_CUDA(b->d_item_task.ensure((size_t)item * 4));
+    if (item)
+        SCRS_CUDA(cudaMemcpy(b->d_item_task.p, b->item_task.data(), (size_t)item * 4, cudaMemcpyHostToDevice));
     b->max_plan_r = max_r;
     if (off > arena_bytes) return set_err(err, SCRS_ERR_CAPACITY, off, arena_bytes);  // layout invariant
     SCRS_CUDA(cudaMemcpy(b->d_arena.p, b->arena.data(), b->arena.size(), cudaMemcpyHostToDevice));
@@ -286,8 +294,8 @@ int32_t enqueue_batch(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
     if (b->total_items) {
         int grid = b->sm_count * mxk_ctas_per_sm(0, (int)b->max_in);
         grid = std::min<int>(grid, (int)b->total_items);
-        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), (uint32_t)b->tasks.size(), b->total_items,
-                                   b->d_counter.as<uint32_t>(), b->status.dev, (int)b->max_in, gf256_strategy(), grid,
+        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), b->total_items,
+                                   b->d_counter.as<uint32_t>(), b->status.dev, (int)b->max_in, grid,
                                    st));
         b->last_launches++;
     }
@@ -349,7 +357,7 @@ extern "C" int32_t scrs_stripe_batch_run_plain(scrs_stripe_batch* b, void* strea
             SCRS_CUDA(launch_cauchy_plan_single(b->plans[pi++], 0, st));
             b->last_launches++;
         }
-        SCRS_CUDA(launch_mxk_single(T, 0, gf256_strategy(), b->status.dev, 0, st));
+        SCRS_CUDA(launch_mxk_single(T, 0, b->status.dev, 0, st));
         b->last_launches++;
     }
     r0 = copy_out(b, st, err);
@@ -373,8 +381,8 @@ extern "C" int32_t scrs_stripe_batch_run_timed(scrs_stripe_batch* b, void* strea
     cudaEventRecord(ev[1], st);
     if (b->total_items) {
         int grid = std::min<int>(b->sm_count * mxk_ctas_per_sm(0, (int)b->max_in), (int)b->total_items);
-        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), (uint32_t)b->tasks.size(), b->total_items,
-                                   b->d_counter.as<uint32_t>(), b->status.dev, (int)b->max_in, gf256_strategy(), grid,
+        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), b->total_items,
+                                   b->d_counter.as<uint32_t>(), b->status.dev, (int)b->max_in, grid,
                                    st));
         b->last_launches++;
     }

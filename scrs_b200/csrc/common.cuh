@@ -36,9 +36,10 @@ constexpr uint16_t kGf16Gen = 0x0108;   // gf65536.rs:26
 // index bits (q2 q1 q0) with the in-byte bit index (s2 s1 s0); the map is an
 // involution, so the same call converts planes back to bytes.  After the call
 // w[s] holds bit s of the 32 bytes.
+// Exchange the bits of b selected by M with the bits of a selected by M << D.
 template <int D, uint32_t M>
 SCRS_HD void delta_swap(uint32_t& a, uint32_t& b) {
-    uint32_t t = ((a >> D) ^ b) & M;
+    const uint32_t t = ((a >> D) ^ b) & M;
     b ^= t;
     a ^= t << D;
 }
@@ -80,9 +81,16 @@ SCRS_HD void bitslice16(uint32_t (&w)[16]) {
 }
 
 // ---- bounded waits -------------------------------------------------------------
-// Every device-side wait gives up after this many polls and reports
-// SCRS_ERR_DEVICE_TIMEOUT through the launch's status word.
-constexpr uint32_t kWaitPollLimit = 1u << 24;
+// Every device-side wait gives up after kWaitLimitNs of global time (checked
+// every 64 polls) and reports SCRS_ERR_DEVICE_TIMEOUT through the launch's
+// status word.
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ void report_status(int32_t* status, int32_t code) {
     if (status) atomicCAS(status, 0, code);
@@ -106,23 +114,32 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
                  : "memory");
 }
 
-// Returns true when the phase with the given parity has completed.
+// Returns true when the phase with the given parity has completed.  A
+// thread whose phase is still open is suspended by the hardware until the
+// phase completes or about kWaitSuspendNs pass, so waiting costs few issue
+// slots.
+constexpr uint32_t kWaitSuspendNs = 20000;
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
-        : "r"(smem_addr(bar)), "r"(parity)
+        : "r"(smem_addr(bar)), "r"(parity), "n"(kWaitSuspendNs)
         : "memory");
     return done != 0;
 }
 
 // Bounded wait: false (and a status report) when the poll budget runs out.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int32_t* status) {
-    for (uint32_t i = 0; i < kWaitPollLimit; i++)
-        if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
+        for (int i = 0; i < 64; i++)
+            if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > kWaitLimitNs) break;
+    }
     report_status(status, SCRS_ERR_DEVICE_TIMEOUT);
     return false;
 }
@@ -136,6 +153,12 @@ __device__ __forceinline__ void tma_load_1d(void* smem_dst, const void* gmem_src
             smem_addr(smem_dst)),
         "l"(gmem_src), "r"(bytes), "r"(smem_addr(bar))
         : "memory");
+}
+
+// Bulk prefetch of [src, src + bytes) into L2 (src 16-byte aligned, bytes a
+// multiple of 16).
+__device__ __forceinline__ void prefetch_l2_bulk(const void* gmem_src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(gmem_src), "r"(bytes) : "memory");
 }
 
 }  // namespace scrs

@@ -14,16 +14,6 @@
 
 using namespace scrs;
 
-namespace scrs {
-int gf256_strategy() {
-    static int s = [] {
-        const char* e = getenv("SCRS_GF256_STRATEGY");
-        return (e && e[0] == '1') ? 1 : 0;
-    }();
-    return s;
-}
-}  // namespace scrs
-
 namespace {
 
 bool is_gf16(int32_t engine) { return engine == SCRS_ENGINE_TOWER || engine == SCRS_ENGINE_AFFT; }
@@ -147,7 +137,7 @@ int32_t run_cauchy_recover(RecipeBufs& rb, int32_t engine, uint32_t k, const std
     T.ld = std::max<uint32_t>(r, 1);
     T.n_items = n_chunks(L, gf16);
     T.aligned = (L % 16 == 0 && aligned16(src) && aligned16(out) && src_stride % 16 == 0) ? 1u : 0u;
-    SCRS_CUDA(launch_mxk_single(T, gf16 ? 1 : 0, gf256_strategy(), status, 0, s));
+    SCRS_CUDA(launch_mxk_single(T, gf16 ? 1 : 0, status, 0, s));
     return SCRS_OK;
 }
 
@@ -317,7 +307,7 @@ int32_t encode_device(const scrs_batch_encoder* e, const uint8_t* d_data, uint8_
     T.ld = (uint32_t)m;
     T.n_items = n_chunks(L, false);
     T.aligned = (L % 16 == 0 && aligned16(d_data) && aligned16(d_rep)) ? 1u : 0u;
-    SCRS_CUDA(launch_mxk_single(T, 0, gf256_strategy(), e->status.dev, 0, st));
+    SCRS_CUDA(launch_mxk_single(T, 0, e->status.dev, 0, st));
     return SCRS_OK;
 }
 
@@ -803,23 +793,41 @@ extern "C" int32_t scrs_batch_decode_into_with_device(scrs_batch_decoder* b, con
     const uint64_t L = b->p.symbol_len;
     cudaStream_t st = (cudaStream_t)stream;
     if (b->lazy) {
+        // codec.rs:219-238 order: count, then each symbol as a push would
+        // check it (range; Dependent -> DuplicateIndex), then finalize's checks.
+        // The rows are read in place through a codeword-index -> row map.
         if (!s->lazy) return set_err(err, SCRS_DECODE_SCRATCH_MISMATCH);
-        if (count != b->p.k) return set_err(err, SCRS_DECODE_WRONG_COUNT, b->p.k, count);
+        const uint64_t k = b->p.k, n = b->p.k + b->p.m;
+        if (count != k) return set_err(err, SCRS_DECODE_WRONG_COUNT, k, count);
         if (count && (!idx || !d_rows)) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
-        scrs_dec_reset(b->lazy);
-        // order the caller's stream work (payload producers) before the copies
-        cudaEvent_t ev;
-        SCRS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        cudaEventRecord(ev, st);
-        cudaStreamWaitEvent(b->lazy->stream.s, ev, 0);
-        cudaEventDestroy(ev);
+        scrs_decoder* d = b->lazy;
+        scrs_dec_reset(d);
+        std::vector<uint16_t> row_of(n, kNoRow);
         for (uint64_t q = 0; q < count; q++) {
-            scrs_push_outcome o;
-            int32_t r = scrs_dec_push_device(b->lazy, idx[q], d_rows + q * L, L, &o, err);
-            if (r) return r;
-            if (o.kind == SCRS_PUSH_DEPENDENT) return set_err(err, SCRS_DECODE_DUPLICATE_INDEX, idx[q]);
+            if (idx[q] >= n) return set_err(err, SCRS_DECODE_INDEX_OUT_OF_RANGE, idx[q], n);
+            if (row_of[idx[q]] != kNoRow) return set_err(err, SCRS_DECODE_DUPLICATE_INDEX, idx[q]);
+            row_of[idx[q]] = (uint16_t)q;
+            d->have[idx[q]] = 1;
         }
-        return scrs_dec_finalize_into_with_device(b->lazy, d_out, out_len, s->lazy, stream, err);
+        d->received = d->distinct = count;
+        int32_t r = finalize_checks(d, out_len, s->lazy, err);
+        if (r) return r;
+        if (!d_out) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
+        if (d->afft) {
+            r = d->afft->decode(d_rows, d->have.data(), d_out, *s->lazy->afft, d->status.dev, st, err,
+                                row_of.data());
+        } else {
+            std::vector<uint16_t> missing, present, repairs;
+            for (uint32_t i = 0; i < k; i++) (d->have[i] ? present : missing).push_back((uint16_t)i);
+            for (uint32_t j = 0; j < b->p.m && repairs.size() < missing.size(); j++)
+                if (d->have[k + j]) repairs.push_back((uint16_t)j);
+            r = run_cauchy_recover(
+                s->lazy->recipe, d->p.engine, (uint32_t)k, missing, repairs, present,
+                [&](uint32_t cw) { return row_of[cw]; }, d_rows, L, d_out, L, d->tower.powers.as<uint16_t>(),
+                d->status.dev, st, err);
+        }
+        if (r) return r;
+        return set_err(err, SCRS_OK);
     }
     if (s->lazy) return set_err(err, SCRS_DECODE_SCRATCH_MISMATCH);
     std::vector<uint16_t> missing, present, repairs, row_of;
@@ -957,7 +965,7 @@ int32_t flush(scrs_incremental_encoder* e, scrs_error* err) {
     T.n_items = n_chunks(L, gf16);
     T.aligned = (L % 16 == 0) ? 1u : 0u;
     T.accumulate = 1;
-    SCRS_CUDA(launch_mxk_single(T, gf16 ? 1 : 0, gf256_strategy(), e->status.dev, 0, st));
+    SCRS_CUDA(launch_mxk_single(T, gf16 ? 1 : 0, e->status.dev, 0, st));
     e->pending.clear();
     std::fill(e->pending_host.begin(), e->pending_host.end(), 0);
     std::fill(e->pending_dev.begin(), e->pending_dev.end(), 0);

@@ -9,6 +9,9 @@
 #pragma once
 
 #include "common.cuh"
+#if defined(__CUDA_ARCH__)
+#include "brx_dispatch.cuh"
+#endif
 
 namespace scrs {
 
@@ -48,7 +51,9 @@ SCRS_HD void mulacc8x2(uint32_t (&acc)[16], const uint32_t (&p)[16]) {
         SCRS_R16(M, 96) SCRS_R16(M, 112) SCRS_R16(M, 128) SCRS_R16(M, 144) SCRS_R16(M, 160)             \
             SCRS_R16(M, 176) SCRS_R16(M, 192) SCRS_R16(M, 208) SCRS_R16(M, 224) SCRS_R16(M, 240)
 
-// Strategy 0: one 256-way jump per coefficient (smallest XOR count).
+// Host reference forms of the multiply (the device code dispatches through
+// the generated jump tables in brx_dispatch.cuh instead).
+// One 256-way switch per coefficient.
 SCRS_HD void mul8_byte(uint32_t c, uint32_t (&acc)[8], const uint32_t (&p)[8]) {
 #define SCRS_CASE8(N) \
     case (N): mulacc8<(N)>(acc, p); break;
@@ -56,7 +61,7 @@ SCRS_HD void mul8_byte(uint32_t c, uint32_t (&acc)[8], const uint32_t (&p)[8]) {
 #undef SCRS_CASE8
 }
 
-// Strategy 1: c = lo + 16*hi, two 16-way jumps (8x less code).
+// c = lo + 16*hi: two 16-way switches.
 SCRS_HD void mul8_nibble(uint32_t c, uint32_t (&acc)[8], const uint32_t (&p)[8]) {
 #define SCRS_CASE8L(N) \
     case (N): mulacc8<(N)>(acc, p); break;
@@ -66,14 +71,6 @@ SCRS_HD void mul8_nibble(uint32_t c, uint32_t (&acc)[8], const uint32_t (&p)[8])
     switch ((c >> 4) & 15u) { SCRS_R16(SCRS_CASE8H, 0) }
 #undef SCRS_CASE8L
 #undef SCRS_CASE8H
-}
-
-template <int kStrategy>
-SCRS_HD void mul8(uint32_t c, uint32_t (&acc)[8], const uint32_t (&p)[8]) {
-    if (kStrategy == 0)
-        mul8_byte(c, acc, p);
-    else
-        mul8_nibble(c, acc, p);
 }
 
 // acc ^= v * x for a GF(256) scalar v applied to both tower components.
@@ -103,9 +100,22 @@ SCRS_HD void mul_by_u(uint32_t (&x)[16]) {
     }
 }
 
+template <bool kUniform>
+SCRS_HD void mul8x2_dispatch(uint32_t v, uint32_t (&acc)[16], const uint32_t (&p)[16]) {
+#if defined(__CUDA_ARCH__)
+    if (kUniform)
+        brx_mul8x2_nib(v & 15u, (v >> 4) & 15u, acc, p);
+    else
+        brx_mul8x2_nib_div(v & 15u, (v >> 4) & 15u, acc, p);
+#else
+    mul8x2_nibble(v, acc, p);
+#endif
+}
+
 // acc ^= c * x over GF((2^8)^2), c = c0 + c1*u:  c*x = c0*x + c1*(u*x).
 // The loop runs the same two jump tables twice (x, then u*x) so the code
-// holds one copy of each.
+// holds one copy of each.  kUniform: c is the same in every lane of the warp.
+template <bool kUniform = true>
 SCRS_HD void mul16(uint32_t c, uint32_t (&acc)[16], const uint32_t (&p)[16]) {
     uint32_t x[16];
 #pragma unroll
@@ -114,7 +124,7 @@ SCRS_HD void mul16(uint32_t c, uint32_t (&acc)[16], const uint32_t (&p)[16]) {
 #pragma unroll 1
     for (int t = 0; t < 2; t++) {
         uint32_t v = t ? c1 : c0;
-        if (v) mul8x2_nibble(v, acc, x);
+        if (v) mul8x2_dispatch<kUniform>(v, acc, x);
         if (t == 0) {
             if (c1 == 0) break;
             mul_by_u(x);

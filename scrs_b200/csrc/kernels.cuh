@@ -12,12 +12,13 @@ constexpr int kThreads = 128;   // 4 warps per CTA
 constexpr int kMaxOutGroup = 64; // outputs computed per pass over the inputs
 
 // Field-dependent geometry: bytes a lane owns and the CTA's column chunk.
+// A GF(256) lane holds two 32-byte plane sets, a GF(2^16) lane one 64-byte set.
 template <int kGf16>
 struct FieldGeom {
-    static constexpr int kLaneBytes = kGf16 ? 64 : 32;
+    static constexpr int kLaneBytes = 64;
     static constexpr int kChunk = 32 * kLaneBytes;     // bytes per row per CTA
     static constexpr int kPieces = kLaneBytes / 16;    // 16-byte pieces per lane
-    static constexpr int kSeg = kGf16 ? 16 : 32;       // input rows staged per segment
+    static constexpr int kSeg = 16;                    // input rows staged per segment
     static constexpr int kElem = kGf16 ? 2 : 1;        // coefficient bytes
 };
 
@@ -64,15 +65,17 @@ struct CauchyPlanTask {
 };
 
 // Launchers (return cudaError_t of the launch).
-cudaError_t launch_gf256_mxk(const MxkTask* tasks, uint32_t n_tasks, uint32_t total_items,
-                             uint32_t* work_counter, int32_t* status, int max_in, int strategy,
-                             int grid, cudaStream_t stream);
-cudaError_t launch_gf16_mxk(const MxkTask* tasks, uint32_t n_tasks, uint32_t total_items,
+// Persistent drain of a work queue: item i belongs to tasks[item_task[i]]
+// (row chunk i - item_begin of that task).  work_counter (zeroed before the
+// launch) hands items out dynamically; nullptr strides items by grid instead.
+cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t total_items,
+                             uint32_t* work_counter, int32_t* status, int max_in, int grid,
+                             cudaStream_t stream);
+cudaError_t launch_gf16_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t total_items,
                             uint32_t* work_counter, int32_t* status, int max_in, int grid,
                             cudaStream_t stream);
 // One task by value; grid <= 0 means one CTA per row chunk.
-cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int strategy, int32_t* status, int grid,
-                              cudaStream_t stream);
+cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream);
 cudaError_t launch_cauchy_plan_single(const CauchyPlanTask& task, int gf16, cudaStream_t stream);
 // max_smem_r: largest r among tasks whose `work` is nullptr.
 cudaError_t launch_cauchy_plan(const CauchyPlanTask* tasks, uint32_t n_tasks, int gf16, uint32_t max_smem_r,

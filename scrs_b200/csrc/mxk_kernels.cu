@@ -1,18 +1,22 @@
 // Multiply-XOR stripe kernels for sm_100a.
 //
-// One CTA (4 warps) owns one column chunk of one stripe: 1 KiB of every row
-// for GF(256), 2 KiB for GF((2^8)^2).  Per segment of input rows:
+// One CTA (4 warps) owns one 2 KiB column chunk of one stripe; every lane
+// owns 64 bytes of each row (two sets of 8 GF(256) bit planes, or one set of
+// 16 GF(2^16) planes).
+// For each segment of up to 16 input rows:
 //   1. one thread issues a TMA bulk copy (cp.async.bulk, no multicast) per
-//      input row into shared memory; all threads wait on one mbarrier;
+//      input row into shared memory; all threads wait on the stage's mbarrier;
 //   2. each warp bit-slices its share of the staged rows in place (and writes
 //      decode's present rows straight through to the output);
 //   3. each warp produces whole output rows: for every input row it reads the
 //      row's planes and applies the warp-uniform coefficient through the
-//      jump-tabled XOR networks, then converts back to bytes and stores.
-// Inputs are read from HBM once and outputs written once, which is the
-// algorithmic traffic (k+m)*L for encode and 2*k*L for decode.  A persistent
-// grid drains a device work queue of (stripe, chunk) items, so thousands of
-// uneven stripes run in one launch.
+//      generated jump tables (brx_dispatch.cuh), then converts back to bytes.
+// A jump whose target changes from one use to the next is the expensive part
+// of a multiply, so nothing else (no memory access) sits on the path from one
+// jump to the next: each warp holds its output's coefficients in registers.
+// Inputs are read from HBM once and outputs written once: the algorithmic
+// traffic is (k+m)*L for encode and 2*k*L for decode.  The persistent form
+// drains a device work queue of (stripe, chunk) items.
 #include <algorithm>
 
 #include "gf_mul_core.cuh"
@@ -22,7 +26,16 @@ namespace scrs {
 
 namespace {
 
-constexpr int kSmemHeader = 128;
+// Shared-memory header: mbarrier (0), item words (8, 12), task descriptor
+// (16), one step list per warp (kStepOffset).
+constexpr int kStepOffset = 128;
+constexpr int kStepBytes = 48;  // 2 * kSeg steps + fold marker + 1 read-ahead
+constexpr int kSmemHeader = kStepOffset + 4 * kStepBytes;
+static_assert(2 * FieldGeom<0>::kSeg + 2 <= kStepBytes, "step list too short");
+static_assert(FieldGeom<0>::kSeg <= 32 && FieldGeom<1>::kSeg <= 32, "one lane per staged row");
+constexpr uint32_t kTaskWords = (sizeof(MxkTask) + 3) / 4;
+static_assert(kTaskWords <= 32, "task descriptor must fit one warp's loads");
+static_assert(16 + kTaskWords * 4 <= kStepOffset, "header too small");
 
 __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
 __device__ __forceinline__ uint32_t umin32(uint32_t a, uint32_t b) { return a < b ? a : b; }
@@ -57,149 +70,289 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-template <int kGf16>
-__device__ __forceinline__ uint32_t piece_pos(int pc, int lane) {
-    return (uint32_t)pc * 512u + 16u * (uint32_t)lane;
-}
-
-template <int kGf16, int kStrategy>
-__device__ __forceinline__ void mul_planes(uint32_t c, uint32_t (&acc)[FieldGeom<kGf16>::kLaneBytes / 4],
-                                           const uint32_t (&p)[FieldGeom<kGf16>::kLaneBytes / 4]) {
-    if constexpr (kGf16)
-        mul16(c, acc, p);
-    else
-        mul8<kStrategy>(c, acc, p);
-}
+// Byte offset of a lane's piece pc (16 bytes) within a chunk row: piece pc
+// of all 32 lanes is one contiguous, coalesced 512-byte span.
+__device__ __forceinline__ uint32_t piece_pos(int pc, int lane) { return (uint32_t)pc * 512u + 16u * (uint32_t)lane; }
 
 template <int kGf16>
-__device__ __forceinline__ void bitslice_lane(uint32_t (&w)[FieldGeom<kGf16>::kLaneBytes / 4]) {
-    if constexpr (kGf16)
+struct Lane {
+    static constexpr int kPieces = FieldGeom<kGf16>::kPieces;
+    static constexpr int kWords = 4 * kPieces;
+    using Words = uint32_t[kWords];
+};
+
+template <int kGf16>
+__device__ __forceinline__ void bitslice_lane(typename Lane<kGf16>::Words& w) {
+    if constexpr (kGf16) {
         bitslice16(w);
-    else
-        bitslice8(w);
+    } else {
+#pragma unroll
+        for (int h = 0; h < Lane<0>::kWords; h += 8) bitslice8(*reinterpret_cast<uint32_t(*)[8]>(&w[h]));
+    }
 }
 
-// Process one (task, chunk) item; returns false on a device wait timeout.
-template <int kGf16, int kStrategy>
-__device__ bool process_item(const MxkTask& T, uint32_t chunk, uint8_t* planes, uint8_t* coef_s, uint64_t* bar,
-                             uint32_t& phase, int seg_cap, int32_t* status) {
+template <int kGf16>
+__device__ __forceinline__ void mul_planes(uint32_t c, typename Lane<kGf16>::Words& acc,
+                                           const typename Lane<kGf16>::Words& p) {
+    if constexpr (kGf16) {
+        mul16<true>(c, acc, p);
+    } else {
+        mul8x2_dispatch<true>(c, acc, p);  // the same coefficient on both plane sets
+    }
+}
+
+template <int kGf16>
+__device__ __forceinline__ void load_lane(const uint8_t* base, int lane, typename Lane<kGf16>::Words& w) {
+#pragma unroll
+    for (int pc = 0; pc < Lane<kGf16>::kPieces; pc++) {
+        uint4 v = *reinterpret_cast<const uint4*>(base + piece_pos(pc, lane));
+        w[4 * pc] = v.x, w[4 * pc + 1] = v.y, w[4 * pc + 2] = v.z, w[4 * pc + 3] = v.w;
+    }
+}
+
+template <int kGf16>
+__device__ __forceinline__ void store_lane(uint8_t* base, int lane, const typename Lane<kGf16>::Words& w) {
+#pragma unroll
+    for (int pc = 0; pc < Lane<kGf16>::kPieces; pc++)
+        *reinterpret_cast<uint4*>(base + piece_pos(pc, lane)) =
+            make_uint4(w[4 * pc], w[4 * pc + 1], w[4 * pc + 2], w[4 * pc + 3]);
+}
+
+// Issue the TMA copies of input rows [seg, seg + seg_n) of one chunk.  Called
+// by all 32 lanes of one warp: lane i < seg_n resolves and copies row seg + i,
+// so the row-number loads overlap instead of following one another.
+template <int kGf16>
+__device__ __forceinline__ void issue_stage(const MxkTask& T, uint32_t chunk, uint32_t seg, uint32_t seg_n,
+                                            uint8_t* buf, uint64_t* bar, int lane) {
     using G = FieldGeom<kGf16>;
-    constexpr int W = G::kLaneBytes / 4;
+    const uint64_t off = (uint64_t)chunk * G::kChunk;
+    const uint32_t bytes = (uint32_t)umin64(G::kChunk, T.L - off);
+    const uint8_t* src = nullptr;
+    if ((uint32_t)lane < seg_n) {
+        const uint32_t r = T.in_rows ? T.in_rows[seg + lane] : seg + lane;
+        src = T.in + (uint64_t)r * T.in_stride + off;
+    }
+    if (lane == 0) mbar_arrive_expect_tx(bar, seg_n * bytes);
+    __syncwarp();
+    if ((uint32_t)lane < seg_n) {
+        fence_proxy_async_smem();
+        tma_load_1d(buf + (size_t)lane * G::kChunk, src, bytes, bar);
+    }
+}
+
+// Whether an item reads any input rows at all.
+__device__ __forceinline__ bool item_loads(const MxkTask& T, uint32_t out_lo, uint32_t out_hi) {
+    return T.n_in && (out_hi > out_lo || (out_lo == 0 && T.pass_rows != nullptr));
+}
+
+// Coefficient of input row seg + lane for output og + j, or 0 past the segment.
+template <int kGf16>
+__device__ __forceinline__ uint32_t lane_coef(const MxkTask& T, uint32_t seg, uint32_t seg_n, uint32_t og, uint32_t j,
+                                              int lane) {
+    if ((uint32_t)lane >= seg_n) return 0;
+    const size_t crow = T.coef_rows ? T.coef_rows[seg + lane] : seg + lane;
+    const size_t src = crow * T.ld + og + j;
+    if constexpr (kGf16)
+        return __ldg(reinterpret_cast<const uint16_t*>(T.coef) + src);
+    else
+        return __ldg(reinterpret_cast<const uint8_t*>(T.coef) + src);
+}
+
+// Store `n` 16-byte pieces starting at piece pc0 of this lane.  `full`: the
+// whole chunk lies inside an aligned row, so no bounds checks are needed.
+template <int kN>
+__device__ __forceinline__ void store_pieces(uint8_t* row, uint64_t off, int pc0, int lane, uint64_t L, bool aligned,
+                                             bool full, const uint32_t* w) {
+    if (full) {
+#pragma unroll
+        for (int q = 0; q < kN; q++)
+            *reinterpret_cast<uint4*>(row + off + piece_pos(pc0 + q, lane)) =
+                make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < kN; q++)
+            store_piece(row, off + piece_pos(pc0 + q, lane), L, aligned,
+                        make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]));
+    }
+}
+
+template <int kGf16>
+__device__ __forceinline__ void load_out_planes(const uint8_t* orow, uint64_t off, int lane, uint64_t L,
+                                                bool aligned, typename Lane<kGf16>::Words& w) {
+#pragma unroll
+    for (int pc = 0; pc < Lane<kGf16>::kPieces; pc++) {
+        const uint4 v = load_piece(orow, off + piece_pos(pc, lane), L, aligned);
+        w[4 * pc] = v.x, w[4 * pc + 1] = v.y, w[4 * pc + 2] = v.z, w[4 * pc + 3] = v.w;
+    }
+    bitslice_lane<kGf16>(w);
+}
+
+// One output row of one chunk: out = XOR_i c_i * x_i over the staged (bit-sliced)
+// rows x_i, plus the row's existing content when `existing` (accumulate mode or
+// the partial sum of earlier segments).  `c` is lane i's coefficient c_i.
+//
+// GF(256): Horner on nibbles, c*x = 16*(hi*x) + lo*x, so the whole sum is
+// 16 * (XOR_i hi_i x_i) + XOR_i lo_i x_i and one 16-way table (v*x for v < 16,
+// the cheapest half of the multiplication table) serves both passes from a
+// single jump site.  The small table stays in the SM's instruction cache; a
+// 256-way or two 16-way tables do not, and their misses cost more than the
+// second pass over the staged rows.  The warp runs a step list: (i << 4) | hi_i
+// for the nonzero high nibbles, a fold marker 0, then (i << 4) | lo_i.
+template <int kGf16>
+__device__ __forceinline__ void output_row(const uint8_t* buf, uint32_t c, uint8_t* steps, uint32_t seg_n, int lane,
+                                           bool existing, uint8_t* orow, uint64_t off, uint64_t L, bool aligned,
+                                           bool full) {
+    using G = FieldGeom<kGf16>;
+    using Words = typename Lane<kGf16>::Words;
+    constexpr int kWords = Lane<kGf16>::kWords;
+    Words acc;
+    if constexpr (kGf16) {
+        if (existing) {
+            load_out_planes<kGf16>(orow, off, lane, L, aligned, acc);
+        } else {
+#pragma unroll
+            for (int t = 0; t < kWords; t++) acc[t] = 0;
+        }
+        for (uint32_t i = 0; i < seg_n; i++) {
+            const uint32_t ci = __shfl_sync(0xFFFFFFFFu, c, i);
+            if (ci == 0) continue;
+            Words p;
+            load_lane<kGf16>(buf + (size_t)i * G::kChunk, lane, p);
+            mul_planes<kGf16>(ci, acc, p);
+        }
+    } else {
+        const uint32_t hi = c >> 4, lo = c & 15u;
+        const uint32_t mh = __ballot_sync(0xFFFFFFFFu, hi != 0), ml = __ballot_sync(0xFFFFFFFFu, lo != 0);
+        const uint32_t below = (1u << lane) - 1u;
+        const uint32_t nh = __popc(mh);
+        if (hi) steps[__popc(mh & below)] = (uint8_t)((lane << 4) | hi);
+        if (lo) steps[nh + 1 + __popc(ml & below)] = (uint8_t)((lane << 4) | lo);
+        if (lane == 0) steps[nh] = 0;
+        __syncwarp();
+        const uint32_t n_steps = nh + 1 + __popc(ml);
+#pragma unroll
+        for (int t = 0; t < kWords; t++) acc[t] = 0;
+        const uint8_t* lane_buf = buf + 16 * lane;
+        uint32_t d = steps[0];
+        for (uint32_t s = 0; s < n_steps; s++) {
+            const uint32_t dn = steps[s + 1];
+            if (d == 0) {  // high nibbles done: acc = 16 * acc, plus the existing content
+#pragma unroll
+                for (int h = 0; h < kWords; h += 8) {
+                    uint32_t t16[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                    mulacc8<16>(t16, *reinterpret_cast<const uint32_t(*)[8]>(&acc[h]));
+#pragma unroll
+                    for (int r = 0; r < 8; r++) acc[h + r] = t16[r];
+                }
+                if (existing) {
+                    Words e;
+                    load_out_planes<kGf16>(orow, off, lane, L, aligned, e);
+#pragma unroll
+                    for (int t = 0; t < kWords; t++) acc[t] ^= e[t];
+                }
+            } else {
+                Words p;
+                const uint8_t* src = lane_buf + (d >> 4) * (uint32_t)G::kChunk;
+#pragma unroll
+                for (int pc = 0; pc < 4; pc++) {
+                    const uint4 v = *reinterpret_cast<const uint4*>(src + pc * 512);
+                    p[4 * pc] = v.x, p[4 * pc + 1] = v.y, p[4 * pc + 2] = v.z, p[4 * pc + 3] = v.w;
+                }
+#if defined(__CUDA_ARCH__)
+                brx_mul8x2_lo(d & 15u, acc, p);
+#endif
+            }
+            d = dn;
+        }
+        __syncwarp();  // the list is rebuilt for the warp's next output row
+    }
+    bitslice_lane<kGf16>(acc);
+    store_pieces<Lane<kGf16>::kPieces>(orow, off, 0, lane, L, aligned, full, acc);
+}
+
+// Process one item: outputs [out_lo, out_hi) of chunk `chunk` of task T.
+// When `first_issued`, the TMA copies of the first stage (segment 0) were
+// already issued into `buf` on `bar`.  Returns false on a wait timeout.
+template <int kGf16>
+__device__ bool process_item(const MxkTask& T, uint32_t chunk, uint8_t* buf, uint8_t* steps_base, uint64_t* bar,
+                             uint32_t& phase, int seg_cap, int32_t* status, uint32_t out_lo, uint32_t out_hi,
+                             bool first_issued) {
+    using G = FieldGeom<kGf16>;
+    constexpr int kPieces = Lane<kGf16>::kPieces;
+    // GF(256) rows are bit-sliced in two independent 32-byte halves per lane,
+    // which balances the work over the 4 warps for any row count.
+    constexpr int kUnitPieces = kGf16 ? kPieces : kPieces / 2;
+    constexpr int kUnitsPerRow = kPieces / kUnitPieces;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint64_t L = T.L;
     const uint64_t off = (uint64_t)chunk * G::kChunk;
-    const uint32_t bytes_here = (uint32_t)umin64(G::kChunk, L - off);
-    const uint32_t n_in = T.n_in, n_out = T.n_out, ld = T.ld;
+    const uint32_t n_in = T.n_in;
     const bool aligned = T.aligned != 0;
+    const bool full = aligned && off + G::kChunk <= L;
+    uint8_t* steps = steps_base + warp * kStepBytes;
 
-    for (uint32_t og = 0; og == 0 || og < n_out; og += kMaxOutGroup) {
-        const uint32_t og_n = n_out > og ? umin32(kMaxOutGroup, n_out - og) : 0;
+    for (uint32_t og = out_lo; og == out_lo || og < out_hi; og += kMaxOutGroup) {
+        const uint32_t og_n = out_hi > og ? umin32(kMaxOutGroup, out_hi - og) : 0;
         const bool need_pass = og == 0 && T.pass_rows != nullptr;
         if (og_n == 0 && !need_pass) break;
         for (uint32_t seg = 0; seg < n_in; seg += seg_cap) {
             const uint32_t seg_n = umin32((uint32_t)seg_cap, n_in - seg);
+            const bool prefetched = first_issued && og == out_lo && seg == 0;
+            // this warp's first output's coefficients, loaded while the rows arrive
+            uint32_t c = (uint32_t)warp < og_n ? lane_coef<kGf16>(T, seg, seg_n, og, warp, lane) : 0u;
             // ---- stage the segment's rows in shared memory
             if (aligned) {
-                if (tid == 0) {
-                    fence_proxy_async_smem();
-                    mbar_arrive_expect_tx(bar, seg_n * bytes_here);
-                    for (uint32_t i = 0; i < seg_n; i++) {
-                        uint32_t r = T.in_rows ? T.in_rows[seg + i] : seg + i;
-                        tma_load_1d(planes + (size_t)i * G::kChunk, T.in + (uint64_t)r * T.in_stride + off,
-                                    bytes_here, bar);
-                    }
-                }
+                if (warp == 0 && !prefetched) issue_stage<kGf16>(T, chunk, seg, seg_n, buf, bar, lane);
                 bool ok = mbar_wait_bounded(bar, phase, status);
                 phase ^= 1u;
                 if (!__syncthreads_and(ok)) return false;
             } else {
                 for (uint32_t i = warp; i < seg_n; i += 4) {
-                    uint32_t r = T.in_rows ? T.in_rows[seg + i] : seg + i;
+                    const uint32_t r = T.in_rows ? T.in_rows[seg + i] : seg + i;
                     const uint8_t* row = T.in + (uint64_t)r * T.in_stride;
 #pragma unroll
-                    for (int pc = 0; pc < G::kPieces; pc++) {
-                        uint32_t pp = piece_pos<kGf16>(pc, lane);
-                        *reinterpret_cast<uint4*>(planes + (size_t)i * G::kChunk + pp) =
-                            load_piece(row, off + pp, L, false);
+                    for (int pc = 0; pc < kPieces; pc++) {
+                        const uint32_t pp = piece_pos(pc, lane);
+                        *reinterpret_cast<uint4*>(buf + (size_t)i * G::kChunk + pp) = load_piece(row, off + pp, L, false);
                     }
                 }
                 __syncthreads();
             }
-            // ---- pass-through copies and in-place bit-slicing
-            for (uint32_t i = warp; i < seg_n; i += 4) {
-                uint8_t* base = planes + (size_t)i * G::kChunk;
-                uint32_t w[W];
+            // ---- pass-through copies and in-place bit-slicing, per (row, half)
+            for (uint32_t u = warp; u < seg_n * kUnitsPerRow; u += 4) {
+                const uint32_t i = u / kUnitsPerRow;
+                const int pc0 = (int)(u - i * kUnitsPerRow) * kUnitPieces;
+                uint8_t* base = buf + (size_t)i * G::kChunk;
+                uint32_t w[4 * kUnitPieces];
 #pragma unroll
-                for (int pc = 0; pc < G::kPieces; pc++) {
-                    uint4 v = *reinterpret_cast<const uint4*>(base + piece_pos<kGf16>(pc, lane));
-                    w[4 * pc] = v.x, w[4 * pc + 1] = v.y, w[4 * pc + 2] = v.z, w[4 * pc + 3] = v.w;
+                for (int q = 0; q < kUnitPieces; q++) {
+                    const uint4 v = *reinterpret_cast<const uint4*>(base + piece_pos(pc0 + q, lane));
+                    w[4 * q] = v.x, w[4 * q + 1] = v.y, w[4 * q + 2] = v.z, w[4 * q + 3] = v.w;
                 }
                 if (need_pass) {
-                    uint16_t pr = T.pass_rows[seg + i];
-                    if (pr != kNoRow) {
-                        uint8_t* orow = T.out + (uint64_t)pr * T.out_stride;
-#pragma unroll
-                        for (int pc = 0; pc < G::kPieces; pc++)
-                            store_piece(orow, off + piece_pos<kGf16>(pc, lane), L, aligned,
-                                        make_uint4(w[4 * pc], w[4 * pc + 1], w[4 * pc + 2], w[4 * pc + 3]));
-                    }
+                    const uint16_t pr = T.pass_rows[seg + i];
+                    if (pr != kNoRow)
+                        store_pieces<kUnitPieces>(T.out + (uint64_t)pr * T.out_stride, off, pc0, lane, L, aligned, full,
+                                                  w);
                 }
                 if (og_n) {
-                    bitslice_lane<kGf16>(w);
+                    if constexpr (kGf16)
+                        bitslice16(*reinterpret_cast<uint32_t(*)[16]>(w));
+                    else
+                        bitslice8(*reinterpret_cast<uint32_t(*)[8]>(w));
 #pragma unroll
-                    for (int pc = 0; pc < G::kPieces; pc++)
-                        *reinterpret_cast<uint4*>(base + piece_pos<kGf16>(pc, lane)) =
-                            make_uint4(w[4 * pc], w[4 * pc + 1], w[4 * pc + 2], w[4 * pc + 3]);
+                    for (int q = 0; q < kUnitPieces; q++)
+                        *reinterpret_cast<uint4*>(base + piece_pos(pc0 + q, lane)) =
+                            make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
                 }
-            }
-            // ---- coefficients of this (output group, segment)
-            for (uint32_t x = tid; x < seg_n * og_n; x += kThreads) {
-                uint32_t i = x / og_n, j = x - i * og_n;
-                size_t crow = T.coef_rows ? T.coef_rows[seg + i] : seg + i;
-                size_t src = crow * ld + og + j;
-                if constexpr (kGf16)
-                    reinterpret_cast<uint16_t*>(coef_s)[x] = reinterpret_cast<const uint16_t*>(T.coef)[src];
-                else
-                    coef_s[x] = reinterpret_cast<const uint8_t*>(T.coef)[src];
             }
             __syncthreads();
             // ---- output rows, one per warp at a time
             for (uint32_t j = warp; j < og_n; j += 4) {
-                uint32_t acc[W];
-                uint32_t orow_idx = T.out_rows ? T.out_rows[og + j] : og + j;
-                uint8_t* orow = T.out + (uint64_t)orow_idx * T.out_stride;
-                if (seg == 0 && !T.accumulate) {
-#pragma unroll
-                    for (int t = 0; t < W; t++) acc[t] = 0;
-                } else {  // existing output (accumulate) or partial sums of earlier segments
-#pragma unroll
-                    for (int pc = 0; pc < G::kPieces; pc++) {
-                        uint4 v = load_piece(orow, off + piece_pos<kGf16>(pc, lane), L, aligned);
-                        acc[4 * pc] = v.x, acc[4 * pc + 1] = v.y, acc[4 * pc + 2] = v.z, acc[4 * pc + 3] = v.w;
-                    }
-                    bitslice_lane<kGf16>(acc);
-                }
-                for (uint32_t i = 0; i < seg_n; i++) {
-                    uint32_t c;
-                    if constexpr (kGf16)
-                        c = reinterpret_cast<const uint16_t*>(coef_s)[i * og_n + j];
-                    else
-                        c = coef_s[i * og_n + j];
-                    if (c == 0) continue;
-                    const uint8_t* base = planes + (size_t)i * G::kChunk;
-                    uint32_t p[W];
-#pragma unroll
-                    for (int pc = 0; pc < G::kPieces; pc++) {
-                        uint4 v = *reinterpret_cast<const uint4*>(base + piece_pos<kGf16>(pc, lane));
-                        p[4 * pc] = v.x, p[4 * pc + 1] = v.y, p[4 * pc + 2] = v.z, p[4 * pc + 3] = v.w;
-                    }
-                    mul_planes<kGf16, kStrategy>(c, acc, p);
-                }
-                bitslice_lane<kGf16>(acc);
-#pragma unroll
-                for (int pc = 0; pc < G::kPieces; pc++)
-                    store_piece(orow, off + piece_pos<kGf16>(pc, lane), L, aligned,
-                                make_uint4(acc[4 * pc], acc[4 * pc + 1], acc[4 * pc + 2], acc[4 * pc + 3]));
+                if (j != (uint32_t)warp) c = lane_coef<kGf16>(T, seg, seg_n, og, j, lane);
+                const uint32_t orow_idx = T.out_rows ? T.out_rows[og + j] : og + j;
+                output_row<kGf16>(buf, c, steps, seg_n, lane, seg != 0 || T.accumulate,
+                                  T.out + (uint64_t)orow_idx * T.out_stride, off, L, aligned, full);
             }
             __syncthreads();
         }
@@ -207,67 +360,96 @@ __device__ bool process_item(const MxkTask& T, uint32_t chunk, uint8_t* planes, 
     return true;
 }
 
-template <int kGf16, int kStrategy>
-__device__ __forceinline__ void mxk_smem_setup(uint8_t* smem, int seg_cap, uint64_t*& bar, uint8_t*& planes,
-                                               uint8_t*& coef_s) {
-    using G = FieldGeom<kGf16>;
-    bar = reinterpret_cast<uint64_t*>(smem);
-    planes = smem + kSmemHeader;
-    coef_s = planes + (size_t)seg_cap * G::kChunk;
-    if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
+// Shared memory: [header: mbarrier | item words | task descriptor | step
+// lists] [staged rows: seg_cap * chunk bytes].
+struct SmemLayout {
+    uint64_t* bar;
+    volatile uint32_t* item;  // [0] the item being processed, [1] the next one
+    uint32_t* task;
+    uint8_t* steps;
+    uint8_t* buf;
+};
+
+template <int kGf16>
+__device__ __forceinline__ SmemLayout layout(uint8_t* smem, int seg_cap) {
+    uint8_t* buf = smem + kSmemHeader;
+    (void)seg_cap;
+    return SmemLayout{reinterpret_cast<uint64_t*>(smem), reinterpret_cast<volatile uint32_t*>(smem + 8),
+                      reinterpret_cast<uint32_t*>(smem + 16), smem + kStepOffset, buf};
 }
 
-template <int kGf16, int kStrategy>
-__global__ void __launch_bounds__(kThreads) mxk_kernel(const MxkTask* __restrict__ tasks, uint32_t n_tasks,
-                                                       uint32_t total_items, uint32_t* work_counter,
-                                                       int32_t* status, int seg_cap) {
+// Persistent drain: items are claimed from work_counter (or strided by grid
+// when it is nullptr) one ahead of use, so the claim's latency is hidden.
+// Warp 0 loads the current item's descriptor and issues its first stage's
+// copies before the CTA meets at the barrier.
+template <int kGf16>
+__global__ void __launch_bounds__(kThreads, 8) mxk_kernel(const MxkTask* __restrict__ tasks,
+                                                          const uint32_t* __restrict__ item_task,
+                                                          uint32_t total_items, uint32_t* work_counter,
+                                                          int32_t* status, int seg_cap) {
     extern __shared__ __align__(128) uint8_t smem[];
-    volatile uint32_t* item_sh = reinterpret_cast<volatile uint32_t*>(smem + 16);
-    uint64_t* bar;
-    uint8_t *planes, *coef_s;
-    mxk_smem_setup<kGf16, kStrategy>(smem, seg_cap, bar, planes, coef_s);
+    const SmemLayout S = layout<kGf16>(smem, seg_cap);
+    const int tid = threadIdx.x;
+    uint32_t claims = 0;
+    auto claim = [&]() -> uint32_t {
+        const uint32_t v = work_counter ? atomicAdd(work_counter, 1u) : blockIdx.x + claims * gridDim.x;
+        claims++;
+        return v;
+    };
+    if (tid == 0) {
+        mbar_init(S.bar, 1);
+        fence_mbar_init();
+        S.item[1] = claim();
+    }
     uint32_t phase = 0;
-    for (uint32_t iter = 0;; iter++) {
-        uint32_t item;
-        if (work_counter) {
-            if (threadIdx.x == 0) *item_sh = atomicAdd(work_counter, 1u);
-            __syncthreads();
-            item = *item_sh;
-        } else {
-            item = blockIdx.x + iter * gridDim.x;
+    for (;;) {
+        if (tid == 0) {
+            const uint32_t cur = S.item[1];
+            S.item[0] = cur;
+            S.item[1] = cur < total_items ? claim() : total_items;
         }
-        if (item >= total_items) break;
-        uint32_t lo = 0, hi = n_tasks - 1;
-        while (lo < hi) {
-            uint32_t mid = (lo + hi + 1) >> 1;
-            if (tasks[mid].item_begin <= item)
-                lo = mid;
-            else
-                hi = mid - 1;
+        __syncthreads();
+        const uint32_t item = S.item[0];
+        if (item >= total_items) return;
+        if (tid < 32) {
+            if (tid < (int)kTaskWords)
+                S.task[tid] = __ldg(reinterpret_cast<const uint32_t*>(tasks + __ldg(item_task + item)) + tid);
+            __syncwarp();
+            const MxkTask& T = *reinterpret_cast<const MxkTask*>(S.task);
+            if (T.aligned && item_loads(T, 0, T.n_out))
+                issue_stage<kGf16>(T, item - T.item_begin, 0, umin32((uint32_t)seg_cap, T.n_in), S.buf, S.bar, tid);
         }
-        const MxkTask T = tasks[lo];
-        if (!process_item<kGf16, kStrategy>(T, item - T.item_begin, planes, coef_s, bar, phase, seg_cap, status))
-            break;
+        __syncthreads();
+        const MxkTask& T = *reinterpret_cast<const MxkTask*>(S.task);
+        const bool issued = T.aligned && item_loads(T, 0, T.n_out);
+        if (!process_item<kGf16>(T, item - T.item_begin, S.buf, S.steps, S.bar, phase, seg_cap, status, 0, T.n_out,
+                                 issued))
+            return;
         __syncthreads();
     }
 }
 
-// One task passed by value (kernel parameter space), CTAs striding over its
-// row chunks: the single-stripe launch used by the per-codec entry points and
-// by the one-launch-per-stripe baseline.
-template <int kGf16, int kStrategy>
-__global__ void __launch_bounds__(kThreads) mxk_single_kernel(const MxkTask T, int32_t* status, int seg_cap) {
+// One task passed by value (kernel parameter space).  Items are (row chunk,
+// output range) with `per` outputs each, so a stripe with few row chunks
+// still spreads over the SMs (the chunk's rows are then staged once per
+// output range, mostly from L2).
+template <int kGf16>
+__global__ void __launch_bounds__(kThreads, 8) mxk_single_kernel(const MxkTask T, int32_t* status,
+                                                                            int seg_cap, uint32_t per) {
     extern __shared__ __align__(128) uint8_t smem[];
-    uint64_t* bar;
-    uint8_t *planes, *coef_s;
-    mxk_smem_setup<kGf16, kStrategy>(smem, seg_cap, bar, planes, coef_s);
+    const SmemLayout S = layout<kGf16>(smem, seg_cap);
+    if (threadIdx.x == 0) {
+        mbar_init(S.bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
     uint32_t phase = 0;
-    for (uint32_t item = blockIdx.x; item < T.n_items; item += gridDim.x) {
-        if (!process_item<kGf16, kStrategy>(T, item, planes, coef_s, bar, phase, seg_cap, status)) break;
+    const uint32_t splits = T.n_out ? (T.n_out + per - 1) / per : 1;
+    const uint32_t items = T.n_items * splits;
+    for (uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
+        const uint32_t chunk = item % T.n_items, sp = item / T.n_items;
+        const uint32_t lo = sp * per, hi = min(T.n_out, lo + per);
+        if (!process_item<kGf16>(T, chunk, S.buf, S.steps, S.bar, phase, seg_cap, status, lo, hi, false)) break;
         __syncthreads();
     }
 }
@@ -418,85 +600,89 @@ cudaError_t ensure_tables() {
     return e;
 }
 
-template <int kGf16, int kStrategy>
+size_t smem_bytes(int gf16, int max_in) {
+    const int chunk = gf16 ? FieldGeom<1>::kChunk : FieldGeom<0>::kChunk;
+    const int segmax = gf16 ? FieldGeom<1>::kSeg : FieldGeom<0>::kSeg;
+    const int elem = gf16 ? 2 : 1;
+    const int seg = std::max(1, std::min(max_in, segmax));
+    (void)elem;
+    return (size_t)kSmemHeader + (size_t)seg * chunk;
+}
+
+template <int kGf16>
 cudaError_t set_mxk_attrs() {
     using G = FieldGeom<kGf16>;
     static bool done = false;
     if (done) return cudaSuccess;
-    int bytes = (int)mxk_smem_bytes(kGf16, G::kSeg);
-    cudaError_t e = cudaFuncSetAttribute(mxk_kernel<kGf16, kStrategy>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    const int smem = (int)smem_bytes(kGf16, G::kSeg);
+    cudaError_t e = cudaFuncSetAttribute(mxk_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(mxk_single_kernel<kGf16, kStrategy>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(mxk_single_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess) done = true;
     return e;
 }
 
-template <int kGf16, int kStrategy>
+template <int kGf16>
 cudaError_t launch_single_impl(const MxkTask& T, int32_t* status, int grid, cudaStream_t stream) {
     using G = FieldGeom<kGf16>;
     if (T.n_items == 0 || (T.n_out == 0 && T.pass_rows == nullptr)) return cudaSuccess;
-    cudaError_t e = set_mxk_attrs<kGf16, kStrategy>();
+    cudaError_t e = set_mxk_attrs<kGf16>();
     if (e != cudaSuccess) return e;
     int seg_cap = std::max(1, std::min((int)T.n_in, G::kSeg));
-    if (grid <= 0 || grid > (int)T.n_items) grid = (int)T.n_items;
-    mxk_single_kernel<kGf16, kStrategy><<<grid, kThreads, mxk_smem_bytes(kGf16, T.n_in), stream>>>(T, status,
-                                                                                                 seg_cap);
+    // Split the outputs when the row chunks alone cannot fill the GPU.
+    constexpr uint32_t kTargetItems = 2 * 148;
+    uint32_t per = std::max<uint32_t>(T.n_out, 1);
+    if (T.n_items < kTargetItems && T.n_out > 1) {
+        uint32_t splits = std::min<uint32_t>(T.n_out, (kTargetItems + T.n_items - 1) / T.n_items);
+        per = (T.n_out + splits - 1) / splits;
+    }
+    const uint32_t items = T.n_items * (T.n_out ? (T.n_out + per - 1) / per : 1);
+    if (grid <= 0 || grid > (int)items) grid = (int)items;
+    mxk_single_kernel<kGf16><<<grid, kThreads, smem_bytes(kGf16, T.n_in), stream>>>(T, status, seg_cap, per);
     return cudaGetLastError();
 }
 
-template <int kGf16, int kStrategy>
-cudaError_t launch_mxk_impl(const MxkTask* tasks, uint32_t n_tasks, uint32_t total_items, uint32_t* counter,
-                            int32_t* status, int max_in, int grid, cudaStream_t stream) {
+template <int kGf16>
+cudaError_t launch_mxk_impl(const MxkTask* tasks, const uint32_t* item_task, uint32_t total_items,
+                            uint32_t* counter, int32_t* status, int max_in, int grid, cudaStream_t stream) {
     using G = FieldGeom<kGf16>;
-    if (total_items == 0 || n_tasks == 0) return cudaSuccess;
+    if (total_items == 0) return cudaSuccess;
     int seg_cap = std::max(1, std::min(max_in, G::kSeg));
-    size_t smem = mxk_smem_bytes(kGf16, max_in);
-    cudaError_t e = set_mxk_attrs<kGf16, kStrategy>();
+    cudaError_t e = set_mxk_attrs<kGf16>();
     if (e != cudaSuccess) return e;
     if (grid <= 0) grid = (int)total_items;
-    mxk_kernel<kGf16, kStrategy><<<grid, kThreads, smem, stream>>>(tasks, n_tasks, total_items, counter, status,
-                                                                     seg_cap);
+    mxk_kernel<kGf16><<<grid, kThreads, smem_bytes(kGf16, max_in), stream>>>(tasks, item_task, total_items,
+                                                                           counter, status, seg_cap);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-size_t mxk_smem_bytes(int gf16, int max_in) {
-    int chunk = gf16 ? FieldGeom<1>::kChunk : FieldGeom<0>::kChunk;
-    int segmax = gf16 ? FieldGeom<1>::kSeg : FieldGeom<0>::kSeg;
-    int elem = gf16 ? 2 : 1;
-    int seg = std::max(1, std::min(max_in, segmax));
-    return (size_t)kSmemHeader + (size_t)seg * chunk + (size_t)seg * kMaxOutGroup * elem;
-}
+size_t mxk_smem_bytes(int gf16, int max_in) { return smem_bytes(gf16, max_in); }
 
 int mxk_ctas_per_sm(int gf16, int max_in) {
     int n = 0;
-    size_t smem = mxk_smem_bytes(gf16, max_in);
-    cudaError_t e = gf16 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mxk_kernel<1, 1>, kThreads, smem)
-                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mxk_kernel<0, 0>, kThreads, smem);
+    if ((gf16 ? set_mxk_attrs<1>() : set_mxk_attrs<0>()) != cudaSuccess) return 1;
+    const size_t smem = smem_bytes(gf16, max_in);
+    cudaError_t e = gf16 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mxk_kernel<1>, kThreads, smem)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mxk_kernel<0>, kThreads, smem);
     if (e != cudaSuccess || n < 1) n = 1;
     return n;
 }
 
-cudaError_t launch_gf256_mxk(const MxkTask* tasks, uint32_t n_tasks, uint32_t total_items, uint32_t* counter,
-                             int32_t* status, int max_in, int strategy, int grid, cudaStream_t stream) {
-    if (strategy == 0)
-        return launch_mxk_impl<0, 0>(tasks, n_tasks, total_items, counter, status, max_in, grid, stream);
-    return launch_mxk_impl<0, 1>(tasks, n_tasks, total_items, counter, status, max_in, grid, stream);
+cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t total_items,
+                             uint32_t* counter, int32_t* status, int max_in, int grid, cudaStream_t stream) {
+    return launch_mxk_impl<0>(tasks, item_task, total_items, counter, status, max_in, grid, stream);
 }
 
-cudaError_t launch_gf16_mxk(const MxkTask* tasks, uint32_t n_tasks, uint32_t total_items, uint32_t* counter,
-                            int32_t* status, int max_in, int grid, cudaStream_t stream) {
-    return launch_mxk_impl<1, 1>(tasks, n_tasks, total_items, counter, status, max_in, grid, stream);
+cudaError_t launch_gf16_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t total_items,
+                            uint32_t* counter, int32_t* status, int max_in, int grid, cudaStream_t stream) {
+    return launch_mxk_impl<1>(tasks, item_task, total_items, counter, status, max_in, grid, stream);
 }
 
-cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int strategy, int32_t* status, int grid,
-                              cudaStream_t stream) {
-    if (gf16) return launch_single_impl<1, 1>(task, status, grid, stream);
-    if (strategy == 0) return launch_single_impl<0, 0>(task, status, grid, stream);
-    return launch_single_impl<0, 1>(task, status, grid, stream);
+cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream) {
+    if (gf16) return launch_single_impl<1>(task, status, grid, stream);
+    return launch_single_impl<0>(task, status, grid, stream);
 }
 
 cudaError_t launch_cauchy_plan_single(const CauchyPlanTask& task, int gf16, cudaStream_t stream) {

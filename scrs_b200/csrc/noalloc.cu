@@ -153,6 +153,6 @@ extern "C" int32_t scrs_gf256_decode_static(int32_t engine, uint64_t k, uint64_t
     T.ld = r ? r : 1;
     T.n_items = n_chunks(L, false);
     T.aligned = (L % 16 == 0 && aligned16(d_rows) && aligned16(d_out)) ? 1u : 0u;
-    SCRS_CUDA(launch_mxk_single(T, 0, gf256_strategy(), nullptr, 0, st));
+    SCRS_CUDA(launch_mxk_single(T, 0, nullptr, 0, st));
     return set_err(err, SCRS_OK);
 }

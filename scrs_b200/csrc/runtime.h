@@ -134,7 +134,4 @@ inline int32_t take_status(StatusWord& st, scrs_error* err) {
     return SCRS_OK;
 }
 
-// GF(256) multiply-XOR dispatch strategy (0: 256-way, 1: nibble); chosen once.
-int gf256_strategy();
-
 }  // namespace scrs

@@ -53,8 +53,8 @@ int main() {
         bitslice8(p);
         bitslice8(acc0);
         bitslice8(acc1);
-        mul8<0>((uint32_t)c, acc0, p);
-        mul8<1>((uint32_t)c, acc1, p);
+        mul8_byte((uint32_t)c, acc0, p);
+        mul8_nibble((uint32_t)c, acc1, p);
         bitslice8(acc0);
         bitslice8(acc1);
         if (memcmp(acc0, expect, 32) || memcmp(acc1, expect, 32)) {
