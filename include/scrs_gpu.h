@@ -327,9 +327,12 @@ SCRS_API int32_t scrs_stripe_batch_set(scrs_stripe_batch* batch,
                               scrs_error* err);
 /* Host-buffer form of scrs_stripe_batch_set: every `in` / `out` pointer is
  * HOST memory (pinned memory gives asynchronous copies).  The batch owns
- * device staging sized at this call; each run then copies inputs in,
- * runs the work and copies outputs back on the run's stream, merging
- * copies of stripes that are contiguous in host memory. */
+ * device staging sized at this call.  Each run cuts the stripes into up to
+ * 16 pieces of about equal input bytes and pipelines them: the inputs of
+ * piece p+1 are copied in and the outputs of piece p-1 copied out (on two
+ * internal streams) while piece p computes; the run's stream waits for the
+ * last copy.  Copies of stripes that are contiguous in host memory are
+ * merged.  use_graph is ignored in this mode. */
 SCRS_API int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* batch,
                                             const scrs_stripe_desc* descs,
                                             uint64_t count, scrs_error* err);

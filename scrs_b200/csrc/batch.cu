@@ -9,6 +9,12 @@
 //           the (stripe, chunk) work queue; optionally replayed as a graph;
 //   run_plain(): the same work as one plan + one multiply-XOR launch per
 //           stripe, the baseline the persistent form is measured against.
+//
+// Host-buffer mode (set_host): the stripes are cut into up to kMaxPieces
+// pieces of about equal input bytes; piece p's host->device copies, its plan
+// and drain launches and its device->host copies run on three streams, so the
+// copies of one piece overlap the compute of the previous one and both copy
+// directions run at once.
 #include <algorithm>
 #include <map>
 #include <memory>
@@ -33,19 +39,34 @@ struct scrs_stripe_batch {
     uint64_t graph_launches = 0;  // kernels in the captured graph
     uint64_t last_launches = 0;
     int sm_count = 0;
+    std::vector<uint32_t> plan_begin;  // plans of stripes before stripe s
     // host-buffer mode
     struct Copy {
         const void* src;
         void* dst;
         size_t bytes;
     };
+    struct Piece {
+        uint32_t item_lo, item_hi, plan_lo, plan_hi;
+        size_t h2d_lo, h2d_hi, d2h_lo, d2h_hi;
+    };
     bool host_mode = false;
     DevBuf stage_in, stage_out;
     std::vector<Copy> h2d, d2h;
+    std::vector<Piece> pieces;
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    std::vector<cudaEvent_t> events;  // start, end, then per piece: copied in, computed
     ~scrs_stripe_batch() {
         if (graph) cudaGraphExecDestroy(graph);
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
+        if (s_in) cudaStreamDestroy(s_in);
+        if (s_out) cudaStreamDestroy(s_out);
     }
 };
+
+namespace {
+constexpr size_t kMaxPieces = 16;  // one work counter each in d_counter
+}
 
 extern "C" int32_t scrs_stripe_batch_create(uint64_t max_stripes, uint64_t max_items, scrs_stripe_batch** out,
                                             scrs_error* err) {
@@ -62,7 +83,7 @@ extern "C" int32_t scrs_stripe_batch_create(uint64_t max_stripes, uint64_t max_i
     SCRS_CUDA(b->status.init());
     SCRS_CUDA(b->d_tasks.ensure(max_stripes * sizeof(MxkTask)));
     SCRS_CUDA(b->d_plans.ensure(max_stripes * sizeof(CauchyPlanTask)));
-    SCRS_CUDA(b->d_counter.ensure(64));
+    SCRS_CUDA(b->d_counter.ensure(kMaxPieces * sizeof(uint32_t)));
     b->tasks.reserve(max_stripes);
     b->plans.reserve(max_stripes);
     *out = b.release();
@@ -129,10 +150,12 @@ extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe
     // ---- tasks
     b->tasks.clear();
     b->plans.clear();
+    b->plan_begin.assign(count + 1, 0);
     size_t off = coef_bytes;  // decode slots follow the coefficient tables
     uint32_t item = 0, max_in = 1, max_r = 0;
     for (uint64_t s = 0; s < count; s++) {
         const scrs_stripe_desc& d = descs[s];
+        b->plan_begin[s] = (uint32_t)b->plans.size();
         MxkTask T{};
         T.in = d.in;
         T.out = d.out;
@@ -199,6 +222,7 @@ extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe
         item += T.n_items;
         b->tasks.push_back(T);
     }
+    b->plan_begin[count] = (uint32_t)b->plans.size();
     b->total_items = item;
     b->max_in = max_in;
     b->item_task.resize(item);
@@ -240,32 +264,71 @@ extern "C" int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* b, const scrs_s
     std::vector<scrs_stripe_desc> dev(descs, descs + count);
     b->h2d.clear();
     b->d2h.clear();
-    size_t oi = 0, oo = 0;
+    // piece boundaries: about equal input bytes per piece
+    const size_t n_pieces = std::min<size_t>(kMaxPieces, std::max<uint64_t>(count, 1));
+    std::vector<uint64_t> cut;  // first stripe of each piece, then count
+    size_t oi = 0, oo = 0, acc = 0;
     for (uint64_t s = 0; s < count; s++) {
         const scrs_stripe_desc& d = descs[s];
         if (!d.in || !d.out) return set_err(err, SCRS_ERR_NULL_ARGUMENT, 0, s);
+        const size_t ib = (size_t)d.k * d.symbol_len;
+        if (cut.empty() || (acc * n_pieces >= in_bytes * cut.size() && cut.size() < n_pieces)) cut.push_back(s);
+        acc += (ib + 15) & ~(size_t)15;
+    }
+    cut.push_back(count);
+    std::vector<size_t> h2d_at, d2h_at;  // copy-list positions of each piece
+    size_t piece = 0;
+    for (uint64_t s = 0; s < count; s++) {
+        const scrs_stripe_desc& d = descs[s];
+        const bool first = s == cut[piece];
+        if (first) {
+            h2d_at.push_back(b->h2d.size());
+            d2h_at.push_back(b->d2h.size());
+        }
         const uint64_t rows_out = d.op == SCRS_OP_ENCODE ? d.m : d.k;
         const size_t ib = (size_t)d.k * d.symbol_len, ob = (size_t)rows_out * d.symbol_len;
         uint8_t* din = b->stage_in.as<uint8_t>() + oi;
         uint8_t* dout = b->stage_out.as<uint8_t>() + oo;
         dev[s].in = din;
         dev[s].out = dout;
-        // merge with the previous copy when both sides are contiguous
-        if (!b->h2d.empty() && (const uint8_t*)b->h2d.back().src + b->h2d.back().bytes == d.in &&
+        // merge with the previous copy of the same piece when both sides are contiguous
+        if (!first && (const uint8_t*)b->h2d.back().src + b->h2d.back().bytes == d.in &&
             (uint8_t*)b->h2d.back().dst + b->h2d.back().bytes == din)
             b->h2d.back().bytes += ib;
         else
             b->h2d.push_back({d.in, din, ib});
-        if (!b->d2h.empty() && (const uint8_t*)b->d2h.back().src + b->d2h.back().bytes == dout &&
+        if (!first && (const uint8_t*)b->d2h.back().src + b->d2h.back().bytes == dout &&
             (uint8_t*)b->d2h.back().dst + b->d2h.back().bytes == d.out)
             b->d2h.back().bytes += ob;
         else
             b->d2h.push_back({dout, d.out, ob});
         oi += (ib + 15) & ~(size_t)15;
         oo += (ob + 15) & ~(size_t)15;
+        if (s + 1 == cut[piece + 1]) piece++;
     }
     int32_t r = scrs_stripe_batch_set(b, dev.data(), count, err);
     if (r) return r;
+    b->pieces.clear();
+    for (size_t q = 0; q + 1 < cut.size(); q++) {
+        const uint64_t s0 = cut[q], s1 = cut[q + 1];
+        scrs_stripe_batch::Piece P{};
+        P.item_lo = b->tasks[s0].item_begin;
+        P.item_hi = s1 < count ? b->tasks[s1].item_begin : b->total_items;
+        P.plan_lo = b->plan_begin[s0];
+        P.plan_hi = b->plan_begin[s1];
+        P.h2d_lo = h2d_at[q];
+        P.h2d_hi = q + 1 < h2d_at.size() ? h2d_at[q + 1] : b->h2d.size();
+        P.d2h_lo = d2h_at[q];
+        P.d2h_hi = q + 1 < d2h_at.size() ? d2h_at[q + 1] : b->d2h.size();
+        b->pieces.push_back(P);
+    }
+    if (!b->s_in) SCRS_CUDA(cudaStreamCreateWithFlags(&b->s_in, cudaStreamNonBlocking));
+    if (!b->s_out) SCRS_CUDA(cudaStreamCreateWithFlags(&b->s_out, cudaStreamNonBlocking));
+    while (b->events.size() < 2 + 2 * kMaxPieces) {
+        cudaEvent_t e;
+        SCRS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        b->events.push_back(e);
+    }
     b->host_mode = true;
     return set_err(err, SCRS_OK);
 }
@@ -294,12 +357,47 @@ int32_t enqueue_batch(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
     if (b->total_items) {
         int grid = b->sm_count * mxk_ctas_per_sm(0, (int)b->max_in);
         grid = std::min<int>(grid, (int)b->total_items);
-        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), b->total_items,
-                                   b->d_counter.as<uint32_t>(), b->status.dev, (int)b->max_in, grid,
-                                   st));
+        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), 0, b->total_items,
+                                   b->d_counter.as<uint32_t>(), b->status.dev, (int)b->max_in, grid, st));
         b->last_launches++;
     }
     return SCRS_OK;
+}
+
+// Host-buffer run: copies and compute of consecutive pieces overlap (see top).
+int32_t run_host(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
+    cudaEvent_t ev_start = b->events[0], ev_end = b->events[1];
+    SCRS_CUDA(cudaEventRecord(ev_start, st));
+    SCRS_CUDA(cudaStreamWaitEvent(b->s_in, ev_start, 0));
+    SCRS_CUDA(cudaStreamWaitEvent(b->s_out, ev_start, 0));
+    SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, kMaxPieces * sizeof(uint32_t), st));
+    const int grid = b->sm_count * mxk_ctas_per_sm(0, (int)b->max_in);
+    b->last_launches = 0;
+    for (size_t q = 0; q < b->pieces.size(); q++) {
+        const scrs_stripe_batch::Piece& P = b->pieces[q];
+        cudaEvent_t ev_in = b->events[2 + 2 * q], ev_done = b->events[3 + 2 * q];
+        for (size_t c = P.h2d_lo; c < P.h2d_hi; c++)
+            SCRS_CUDA(cudaMemcpyAsync(b->h2d[c].dst, b->h2d[c].src, b->h2d[c].bytes, cudaMemcpyHostToDevice, b->s_in));
+        SCRS_CUDA(cudaEventRecord(ev_in, b->s_in));
+        SCRS_CUDA(cudaStreamWaitEvent(st, ev_in, 0));
+        if (P.plan_hi > P.plan_lo) {
+            SCRS_CUDA(launch_cauchy_plan(b->d_plans.as<CauchyPlanTask>() + P.plan_lo, P.plan_hi - P.plan_lo, 0,
+                                         b->max_plan_r, st));
+            b->last_launches++;
+        }
+        if (P.item_hi > P.item_lo) {
+            SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), P.item_lo, P.item_hi,
+                                       b->d_counter.as<uint32_t>() + q, b->status.dev, (int)b->max_in, grid, st));
+            b->last_launches++;
+        }
+        SCRS_CUDA(cudaEventRecord(ev_done, st));
+        SCRS_CUDA(cudaStreamWaitEvent(b->s_out, ev_done, 0));
+        for (size_t c = P.d2h_lo; c < P.d2h_hi; c++)
+            SCRS_CUDA(cudaMemcpyAsync(b->d2h[c].dst, b->d2h[c].src, b->d2h[c].bytes, cudaMemcpyDeviceToHost, b->s_out));
+    }
+    SCRS_CUDA(cudaEventRecord(ev_end, b->s_out));
+    SCRS_CUDA(cudaStreamWaitEvent(st, ev_end, 0));
+    return set_err(err, SCRS_OK);
 }
 
 }  // namespace
@@ -307,6 +405,7 @@ int32_t enqueue_batch(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
 extern "C" int32_t scrs_stripe_batch_run(scrs_stripe_batch* b, void* stream, int32_t use_graph, scrs_error* err) {
     if (!b) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
     cudaStream_t st = (cudaStream_t)stream;
+    if (b->host_mode) return run_host(b, st, err);  // pipelined copies; no graph
     int32_t r0 = copy_in(b, st, err);
     if (r0) return r0;
     if (!use_graph) {
@@ -381,9 +480,8 @@ extern "C" int32_t scrs_stripe_batch_run_timed(scrs_stripe_batch* b, void* strea
     cudaEventRecord(ev[1], st);
     if (b->total_items) {
         int grid = std::min<int>(b->sm_count * mxk_ctas_per_sm(0, (int)b->max_in), (int)b->total_items);
-        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), b->total_items,
-                                   b->d_counter.as<uint32_t>(), b->status.dev, (int)b->max_in, grid,
-                                   st));
+        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), 0, b->total_items,
+                                   b->d_counter.as<uint32_t>(), b->status.dev, (int)b->max_in, grid, st));
         b->last_launches++;
     }
     cudaEventRecord(ev[2], st);

@@ -65,20 +65,19 @@ struct CauchyPlanTask {
 };
 
 // Launchers (return cudaError_t of the launch).
-// Persistent drain of a work queue: item i belongs to tasks[item_task[i]]
-// (row chunk i - item_begin of that task).  work_counter (zeroed before the
-// launch) hands items out dynamically; nullptr strides items by grid instead.
-cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t total_items,
-                             uint32_t* work_counter, int32_t* status, int max_in, int grid,
-                             cudaStream_t stream);
-cudaError_t launch_gf16_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t total_items,
-                            uint32_t* work_counter, int32_t* status, int max_in, int grid,
-                            cudaStream_t stream);
+// Persistent drain of the work items [item_lo, item_end): item i belongs to
+// tasks[item_task[i]] (row chunk i - item_begin of that task).  work_counter
+// (zeroed before the launch) hands items out dynamically; nullptr strides
+// items by grid instead.
+cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
+                             uint32_t* work_counter, int32_t* status, int max_in, int grid, cudaStream_t stream);
+cudaError_t launch_gf16_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
+                            uint32_t* work_counter, int32_t* status, int max_in, int grid, cudaStream_t stream);
 // One task by value; grid <= 0 means one CTA per row chunk.
 cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream);
 cudaError_t launch_cauchy_plan_single(const CauchyPlanTask& task, int gf16, cudaStream_t stream);
-// max_smem_r: largest r among tasks whose `work` is nullptr.
-cudaError_t launch_cauchy_plan(const CauchyPlanTask* tasks, uint32_t n_tasks, int gf16, uint32_t max_smem_r,
+// max_r: the largest r among the tasks (all of them, with or without `work`).
+cudaError_t launch_cauchy_plan(const CauchyPlanTask* tasks, uint32_t n_tasks, int gf16, uint32_t max_r,
                                cudaStream_t stream);
 // Largest r the plan kernel keeps in shared memory.
 constexpr uint32_t kPlanSmemMaxR = 12288;

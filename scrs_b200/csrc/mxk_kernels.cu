@@ -385,14 +385,14 @@ __device__ __forceinline__ SmemLayout layout(uint8_t* smem, int seg_cap) {
 template <int kGf16>
 __global__ void __launch_bounds__(kThreads, 8) mxk_kernel(const MxkTask* __restrict__ tasks,
                                                           const uint32_t* __restrict__ item_task,
-                                                          uint32_t total_items, uint32_t* work_counter,
-                                                          int32_t* status, int seg_cap) {
+                                                          uint32_t item_lo, uint32_t total_items,
+                                                          uint32_t* work_counter, int32_t* status, int seg_cap) {
     extern __shared__ __align__(128) uint8_t smem[];
     const SmemLayout S = layout<kGf16>(smem, seg_cap);
     const int tid = threadIdx.x;
     uint32_t claims = 0;
     auto claim = [&]() -> uint32_t {
-        const uint32_t v = work_counter ? atomicAdd(work_counter, 1u) : blockIdx.x + claims * gridDim.x;
+        const uint32_t v = item_lo + (work_counter ? atomicAdd(work_counter, 1u) : blockIdx.x + claims * gridDim.x);
         claims++;
         return v;
     };
@@ -583,10 +583,88 @@ __global__ void __launch_bounds__(256) cauchy_plan_single(const CauchyPlanTask P
     cauchy_plan_body<kGf16>(P);
 }
 
-bool g_tables_uploaded = false;
+// Batched plans with r <= kWarpPlanMaxR: one warp per decode (a whole CTA per
+// decode leaves most of its threads idle when r is a handful).  The same
+// closed form as cauchy_plan_body; rv/cv/rf/cf live in per-warp shared
+// scratch.
+constexpr uint32_t kWarpPlanMaxR = 64;
+constexpr int kPlanWarps = 8;
+
+template <int kGf16>
+__global__ void __launch_bounds__(32 * kPlanWarps) cauchy_plan_warp_kernel(const CauchyPlanTask* __restrict__ tasks,
+                                                                          uint32_t n_tasks) {
+    __shared__ Gf8Tables tb;
+    __shared__ uint32_t scratch[kPlanWarps][4 * kWarpPlanMaxR];
+    for (int i = threadIdx.x; i < 512; i += blockDim.x) {
+        if (i < 256) tb.log[i] = c_gf8_log[i];
+        tb.exp[i] = c_gf8_exp[i % 255];
+    }
+    __syncthreads();
+    FieldOps<kGf16> F{tb};
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint32_t* rv = scratch[wib];
+    uint32_t* cv = rv + kWarpPlanMaxR;
+    uint32_t* rf = rv + 2 * kWarpPlanMaxR;
+    uint32_t* cf = rv + 3 * kWarpPlanMaxR;
+    for (uint32_t t = blockIdx.x * kPlanWarps + wib; t < n_tasks; t += gridDim.x * kPlanWarps) {
+        const CauchyPlanTask P = tasks[t];
+        const uint32_t r = P.r;
+        for (uint32_t u = lane; u < r; u += 32) {
+            rv[u] = y_var<kGf16>(P, tb, P.repairs[u]);
+            cv[u] = x_var<kGf16>(P, tb, P.missing[u]);
+        }
+        __syncwarp();
+        for (uint32_t u = lane; u < 2 * r; u += 32) {
+            const bool is_row = u < r;
+            const uint32_t q = is_row ? u : u - r;
+            const uint32_t v = is_row ? rv[q] : cv[q];
+            const uint32_t* other = is_row ? cv : rv;
+            const uint32_t* same = is_row ? rv : cv;
+            uint32_t cross = 1, within = 1;
+            for (uint32_t h = 0; h < r; h++) {
+                cross = F.mul(cross, v ^ other[h]);
+                if (h != q) within = F.mul(within, v ^ same[h]);
+            }
+            (is_row ? rf : cf)[q] = F.mul(cross, F.inv(within));
+        }
+        __syncwarp();
+        const uint32_t ld = P.ld;
+        for (uint32_t x = lane; x < r * r; x += 32) {
+            const uint32_t a = x / r, b = x - a * r;  // input row a (repair), output b (missing)
+            const uint32_t val = F.mul(F.mul(rf[a], cf[b]), F.inv(cv[b] ^ rv[a]));
+            if (kGf16)
+                reinterpret_cast<uint16_t*>(P.coef)[(size_t)a * ld + b] = (uint16_t)val;
+            else
+                reinterpret_cast<uint8_t*>(P.coef)[(size_t)a * ld + b] = (uint8_t)val;
+        }
+        for (uint32_t x = lane; x < P.p * r; x += 32) {
+            const uint32_t z = x / r, b = x - z * r;  // present row z, output b
+            const uint32_t zv = x_var<kGf16>(P, tb, P.present[z]);
+            uint32_t rp = 1, cp = 1;
+            for (uint32_t h = 0; h < r; h++) {
+                rp = F.mul(rp, zv ^ rv[h]);
+                cp = F.mul(cp, zv ^ cv[h]);
+            }
+            const uint32_t val = F.mul(F.mul(F.mul(cp, F.inv(rp)), cf[b]), F.inv(zv ^ cv[b]));
+            const size_t at = (size_t)(r + z) * ld + b;
+            if (kGf16)
+                reinterpret_cast<uint16_t*>(P.coef)[at] = (uint16_t)val;
+            else
+                reinterpret_cast<uint8_t*>(P.coef)[at] = (uint8_t)val;
+        }
+        __syncwarp();  // scratch is reused by the warp's next decode
+    }
+}
+
+// Constant tables are per device: upload once on each device used.
+bool g_tables_uploaded[64] = {};
 
 cudaError_t ensure_tables() {
-    if (g_tables_uploaded) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e0 = cudaGetDevice(&dev);
+    if (e0 != cudaSuccess) return e0;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (g_tables_uploaded[dev]) return cudaSuccess;
     uint8_t ex[255], lg[256] = {0};
     uint8_t v = 1;
     for (int i = 0; i < 255; i++) {
@@ -596,7 +674,7 @@ cudaError_t ensure_tables() {
     }
     cudaError_t e = cudaMemcpyToSymbol(c_gf8_exp, ex, sizeof ex);
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_gf8_log, lg, sizeof lg);
-    if (e == cudaSuccess) g_tables_uploaded = true;
+    if (e == cudaSuccess) g_tables_uploaded[dev] = true;
     return e;
 }
 
@@ -643,15 +721,15 @@ cudaError_t launch_single_impl(const MxkTask& T, int32_t* status, int grid, cuda
 }
 
 template <int kGf16>
-cudaError_t launch_mxk_impl(const MxkTask* tasks, const uint32_t* item_task, uint32_t total_items,
+cudaError_t launch_mxk_impl(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
                             uint32_t* counter, int32_t* status, int max_in, int grid, cudaStream_t stream) {
     using G = FieldGeom<kGf16>;
-    if (total_items == 0) return cudaSuccess;
+    if (item_end <= item_lo) return cudaSuccess;
     int seg_cap = std::max(1, std::min(max_in, G::kSeg));
     cudaError_t e = set_mxk_attrs<kGf16>();
     if (e != cudaSuccess) return e;
-    if (grid <= 0) grid = (int)total_items;
-    mxk_kernel<kGf16><<<grid, kThreads, smem_bytes(kGf16, max_in), stream>>>(tasks, item_task, total_items,
+    if (grid <= 0 || grid > (int)(item_end - item_lo)) grid = (int)(item_end - item_lo);
+    mxk_kernel<kGf16><<<grid, kThreads, smem_bytes(kGf16, max_in), stream>>>(tasks, item_task, item_lo, item_end,
                                                                            counter, status, seg_cap);
     return cudaGetLastError();
 }
@@ -670,14 +748,14 @@ int mxk_ctas_per_sm(int gf16, int max_in) {
     return n;
 }
 
-cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t total_items,
+cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
                              uint32_t* counter, int32_t* status, int max_in, int grid, cudaStream_t stream) {
-    return launch_mxk_impl<0>(tasks, item_task, total_items, counter, status, max_in, grid, stream);
+    return launch_mxk_impl<0>(tasks, item_task, item_lo, item_end, counter, status, max_in, grid, stream);
 }
 
-cudaError_t launch_gf16_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t total_items,
+cudaError_t launch_gf16_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
                             uint32_t* counter, int32_t* status, int max_in, int grid, cudaStream_t stream) {
-    return launch_mxk_impl<1>(tasks, item_task, total_items, counter, status, max_in, grid, stream);
+    return launch_mxk_impl<1>(tasks, item_task, item_lo, item_end, counter, status, max_in, grid, stream);
 }
 
 cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream) {
@@ -702,12 +780,20 @@ cudaError_t launch_cauchy_plan_single(const CauchyPlanTask& task, int gf16, cuda
     return cudaGetLastError();
 }
 
-cudaError_t launch_cauchy_plan(const CauchyPlanTask* tasks, uint32_t n_tasks, int gf16, uint32_t max_smem_r,
+cudaError_t launch_cauchy_plan(const CauchyPlanTask* tasks, uint32_t n_tasks, int gf16, uint32_t max_r,
                                cudaStream_t stream) {
     if (n_tasks == 0) return cudaSuccess;
     cudaError_t e = ensure_tables();
     if (e != cudaSuccess) return e;
-    size_t smem = (size_t)4 * max_smem_r * sizeof(uint32_t);
+    if (max_r <= kWarpPlanMaxR) {
+        const uint32_t grid = std::min<uint32_t>((n_tasks + kPlanWarps - 1) / kPlanWarps, 148u * 8u);
+        if (gf16)
+            cauchy_plan_warp_kernel<1><<<grid, 32 * kPlanWarps, 0, stream>>>(tasks, n_tasks);
+        else
+            cauchy_plan_warp_kernel<0><<<grid, 32 * kPlanWarps, 0, stream>>>(tasks, n_tasks);
+        return cudaGetLastError();
+    }
+    size_t smem = (size_t)4 * std::min(max_r, kPlanSmemMaxR) * sizeof(uint32_t);
     if (smem > 48 * 1024) {
         auto fn = gf16 ? cauchy_plan_kernel<1> : cauchy_plan_kernel<0>;
         e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
