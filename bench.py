@@ -387,6 +387,89 @@ def extra_latency(torch, api):
     return res
 
 
+def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C250005):
+    """Config 5: Poisson arrivals of mixed encode/decode requests over all four
+    engines through the serving loop (scrs_server_*), 64 GB budget, 8 slots.
+    The rate sweep is 0.3x, 0.6x and 0.9x the closed-loop capacity measured
+    first.  Payloads are seeded random device bytes (decode requests decode
+    random received rows: the same work; bit-exactness is covered by the
+    serving tests).  Latency = completion seen by the host - submit."""
+    from scrs_b200.api import Engine
+    from scrs_b200.serving import OP_DECODE, OP_ENCODE, Server
+
+    rng = np.random.default_rng(seed)
+    tower = [(64, 16, 4096), (256, 64, 1024), (1024, 256, 512), (32, 8, 65536)]
+    afft = [(1024, 1024, 1024), (4096, 4096, 256), (3000, 500, 2048), (16384, 16384, 256)]
+    templates = []
+    for t in range(n_templates):
+        u = rng.random()
+        if u < 0.7:
+            engine = Engine.STANDARD_CAUCHY if rng.random() < 0.5 else Engine.GOOD_CAUCHY
+            k = int(rng.integers(4, 65))
+            m = int(rng.integers(1, 17))
+            Ls = int(rng.choice([1024, 4096, 16384, 65536]))
+        elif u < 0.85:
+            engine = Engine.TOWER
+            k, m, Ls = tower[int(rng.integers(0, len(tower)))]
+        else:
+            engine = Engine.AFFT
+            k, m, Ls = afft[int(rng.integers(0, len(afft)))]
+        op = OP_ENCODE if rng.random() < 0.5 else OP_DECODE
+        d_in = torch.randint(0, 256, (k * Ls,), dtype=torch.uint8, device="cuda")
+        d_out = torch.empty(((m if op == OP_ENCODE else k) * Ls,), dtype=torch.uint8, device="cuda")
+        idx = None
+        if op == OP_DECODE:
+            e = int(rng.integers(0, min(k, m) + 1))
+            erased = set(rng.choice(k, e, replace=False).tolist()) if e else set()
+            idx = [i for i in range(k) if i not in erased] + [k + j for j in rng.choice(m, e, replace=False).tolist()]
+        templates.append((op, engine, k, m, Ls, d_in, d_out, idx))
+    srv = Server(api.lib, 64 << 30, slots=8)
+
+    def submit(t, tag):
+        op, engine, k, m, Ls, d_in, d_out, idx = templates[t]
+        srv.submit(op, engine, k, m, Ls, d_in.data_ptr(), d_out.data_ptr(), idx, tag=tag)
+
+    # warm the resident engines, then the closed-loop capacity
+    for t in range(len(templates)):
+        submit(t, t)
+    srv.drain(600)
+    order = rng.integers(0, len(templates), 2000)
+    t0 = time.perf_counter()
+    for i, t in enumerate(order):
+        submit(int(t), int(t))
+    srv.drain(600)
+    cap_s = time.perf_counter() - t0
+    cap_rate = len(order) / cap_s
+    cap_bytes = sum(templates[int(t)][2] * templates[int(t)][4] for t in order)
+    res = {"workload": "Poisson arrivals; 70% GF(256) (Standard/Good, k~U[4,64], m~U[1,16], L in {1,4,16,64} KiB), "
+                       "15% tower (k<=1024, m<=256), 15% AFFT (k<=16384, m<=16384, L 256-2048); half encode, half "
+                       "decode with random erasures <= m; 64 GB budget, 8 slots, GF(256) coalesced per slot",
+           "closed_loop": {"requests_per_s": round(cap_rate, 1), "goodput_GBps": round(cap_bytes / cap_s / 1e9, 2)},
+           "rates": []}
+    for frac in (0.3, 0.6, 0.9):
+        rate = frac * cap_rate
+        n = int(rate * seconds_per_rate)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+        picks = rng.integers(0, len(templates), n)
+        done, i = [], 0
+        t0 = time.perf_counter()
+        while i < n or srv.pending:
+            now = time.perf_counter() - t0
+            while i < n and arrivals[i] <= now:
+                submit(int(picks[i]), int(picks[i]))
+                i += 1
+            done += srv.progress()
+        el = time.perf_counter() - t0
+        lat = np.array([c.latency_ms for c in done])
+        gb = sum(templates[c.tag][2] * templates[c.tag][4] for c in done)
+        res["rates"].append({"offered_per_s": round(rate, 1), "requests": n, "failed": int(sum(c.status != 0 for c in done)),
+                             "goodput_GBps": round(gb / el / 1e9, 2), "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                             "p99_ms": round(float(np.percentile(lat, 99)), 3)})
+    res["stats"] = srv.stats()
+    srv.close()
+    return res
+
+
 def extra_tower(torch, api):
     """Config 2: Tower k=32 m=8 L=65536, incremental encode (32 feeds) + lazy decode (8 data erased)."""
     from scrs_b200.api import Engine
@@ -553,7 +636,7 @@ def run_ours(args, world, rank, local):
     extras = {}
     if rank == 0 and not args.no_extras:
         for name, fn in (("batched_vs_plain_cfg4", extra_mixed), ("latency_cfg1", extra_latency),
-                         ("tower_cfg2", extra_tower), ("afft_cfg3", extra_afft)):
+                         ("tower_cfg2", extra_tower), ("afft_cfg3", extra_afft), ("serving_cfg5", extra_serving)):
             try:
                 extras[name] = fn(torch, api)
             except Exception as ex:  # reported, never hidden

@@ -357,6 +357,56 @@ SCRS_API int32_t scrs_stripe_batch_run_timed(scrs_stripe_batch* batch, void* str
  * failure a kernel recorded (SCRS_ERR_DEVICE_TIMEOUT). */
 SCRS_API int32_t scrs_stripe_batch_check(scrs_stripe_batch* batch, scrs_error* err);
 
+/* ---- Serving loop (continuous batching) ----------------------------------
+ * No reference counterpart: a request loop over the engines above.  Requests
+ * of every engine are submitted with device-resident inputs and outputs and
+ * admitted first come, first served as one of `slots` streams and the device
+ * memory budget free up; admitted work overlaps on the device.  Waiting
+ * GF(256) requests are coalesced into one stripe batch per slot; tower and
+ * additive-FFT requests take a slot each and use engines kept resident per
+ * slot (least recently used profiles are evicted).  The budget counts every
+ * admitted request's input and output bytes plus estimated resident engine
+ * workspaces.  Results are identical to running each request alone. */
+typedef struct scrs_server scrs_server;
+typedef struct scrs_request {
+    int32_t op;          /* SCRS_OP_ENCODE or SCRS_OP_DECODE                    */
+    int32_t engine;      /* SCRS_ENGINE_*                                       */
+    uint64_t k, m, symbol_len;
+    const uint8_t* in;   /* device: encode k*L data; decode k received rows,
+                            row q holding codeword index indices[q]             */
+    uint8_t* out;        /* device: encode m*L repairs; decode k*L data        */
+    const uint64_t* indices; /* host, decode only: k indices (copied at submit) */
+    uint64_t tag;        /* returned with the completion                       */
+} scrs_request;
+typedef struct scrs_completion {
+    uint64_t ticket, tag;
+    int32_t status;      /* SCRS_OK or the request's error                      */
+    int32_t reserved;
+    uint64_t submit_ns, done_ns; /* host steady clock: submit, completion seen */
+} scrs_completion;
+typedef struct scrs_server_stats {
+    uint64_t submitted, admitted, completed, failed, batches;
+    uint64_t memory_in_use, resident_bytes;
+} scrs_server_stats;
+/* memory_budget in bytes; 1 <= slots <= 64. */
+SCRS_API int32_t scrs_server_create(uint64_t memory_budget, uint32_t slots,
+                                    scrs_server** out, scrs_error* err);
+/* Waits for in-flight work, then frees everything. */
+SCRS_API void scrs_server_destroy(scrs_server* server);
+/* Validates (profile, decode indices, budget: SCRS_ERR_CAPACITY when the
+ * request alone exceeds it), queues, and admits what fits.  Buffers must
+ * stay valid until the request's completion is returned. */
+SCRS_API int32_t scrs_server_submit(scrs_server* server, const scrs_request* req,
+                                    uint64_t* ticket, scrs_error* err);
+/* Non-blocking: retires finished slots, admits waiting requests and returns
+ * up to `capacity` completions in `done` (count in *n_done). */
+SCRS_API int32_t scrs_server_progress(scrs_server* server, scrs_completion* done,
+                                      uint32_t capacity, uint32_t* n_done,
+                                      scrs_error* err);
+/* Requests queued, running or completed but not yet returned. */
+SCRS_API uint64_t scrs_server_pending(const scrs_server* server);
+SCRS_API int32_t scrs_server_get_stats(const scrs_server* server, scrs_server_stats* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1031,3 +1031,16 @@ extern "C" void scrs_inc_reset(scrs_incremental_encoder* e) {
     e->pending.clear();
     e->fed_count = 0;
 }
+
+// Device-side status of a handle's last asynchronous work (used by the
+// serving loop after its completion event fires).
+namespace scrs {
+int32_t internal_batch_encoder_status(scrs_batch_encoder* e, scrs_error* err) {
+    return take_status(e->status, err);
+}
+int32_t internal_batch_decoder_status(scrs_batch_decoder* b, scrs_error* err) {
+    int32_t r = take_status(b->status, err);
+    if (!r && b->lazy) r = take_status(b->lazy->status, err);
+    return r;
+}
+}  // namespace scrs

@@ -1,0 +1,110 @@
+"""The serving loop (scrs_server_*): every request's result is identical when
+it runs alone and when it runs in a mix of overlapping requests of all four
+engines, and equals the oracle's result; admission waits for memory under a
+small budget; a request larger than the budget is refused at submit."""
+import numpy as np
+import pytest
+
+from scrs_b200.api import ConfigError, DecodeError, Engine, RuntimeFailure
+
+from scenarios import encode_word
+
+pytestmark = pytest.mark.gpu
+
+OP_ENCODE, OP_DECODE = 0, 1
+
+
+def make_requests(torch, oracle, seed=11):
+    """(op, engine, k, m, L, input tensor, indices, expected bytes) for a mix
+    of engines, sizes and erasure patterns."""
+    rng = np.random.default_rng(seed)
+    shapes = [(Engine.GOOD_CAUCHY, 10, 4, 4096), (Engine.STANDARD_CAUCHY, 6, 3, 1000),
+              (Engine.GOOD_CAUCHY, 40, 16, 2048), (Engine.STANDARD_CAUCHY, 3, 2, 64),
+              (Engine.TOWER, 8, 4, 1024), (Engine.TOWER, 32, 8, 4096),
+              (Engine.AFFT, 64, 64, 256), (Engine.AFFT, 100, 28, 512)]
+    reqs = []
+    for rep in range(3):
+        for engine, k, m, L in shapes:
+            p = oracle.resolve(engine, k, m, L)
+            data = rng.integers(0, 256, k * L, dtype=np.uint8)
+            word = encode_word(oracle, p, data)
+            if (rep + k) % 2 == 0:
+                reqs.append((OP_ENCODE, engine, k, m, L, torch.from_numpy(data).cuda(), None,
+                             np.concatenate(word[k:])))
+            else:
+                e = int(rng.integers(0, min(k, m) + 1))
+                erased = set(rng.choice(k, e, replace=False).tolist())
+                extra = rng.choice(m, e, replace=False).tolist()
+                idx = [i for i in range(k) if i not in erased] + [k + j for j in extra]
+                idx = rng.permutation(idx).tolist()
+                rows = torch.from_numpy(np.concatenate([word[i] for i in idx])).cuda()
+                reqs.append((OP_DECODE, engine, k, m, L, rows, idx, data))
+    return reqs
+
+
+def run(server, torch, reqs, order):
+    outs = [None] * len(reqs)
+    for q in order:
+        op, engine, k, m, L, d_in, idx, exp = reqs[q]
+        outs[q] = torch.full((len(exp),), 0xAB, dtype=torch.uint8, device="cuda")
+        server.submit(op, engine, k, m, L, d_in.data_ptr(), outs[q].data_ptr(), idx, tag=q)
+    done = server.drain()
+    assert sorted(c.tag for c in done) == sorted(order)
+    assert all(c.status == 0 for c in done), [c.status for c in done]
+    assert all(c.done_ns >= c.submit_ns for c in done)
+    torch.cuda.synchronize()
+    return outs
+
+
+def test_results_alone_and_in_mix_match(gpu, oracle):
+    torch = pytest.importorskip("torch")
+    from scrs_b200.serving import Server
+
+    reqs = make_requests(torch, oracle)
+    srv = Server(gpu.lib, 1 << 30, slots=4)
+    alone = []
+    for q in range(len(reqs)):  # each request alone: submit, then wait for it
+        alone.append(run(srv, torch, reqs, [q])[q])
+    order = np.random.default_rng(3).permutation(len(reqs)).tolist()
+    mixed = run(srv, torch, reqs, order)  # all at once: admitted as slots free up
+    for q, r in enumerate(reqs):
+        exp = r[-1]
+        assert np.array_equal(alone[q].cpu().numpy(), exp), q
+        assert np.array_equal(mixed[q].cpu().numpy(), exp), q
+    st = srv.stats()
+    assert st["completed"] == 2 * len(reqs) and st["failed"] == 0
+    assert st["batches"] >= 1
+    srv.close()
+
+
+def test_small_budget_queues_and_completes(gpu, oracle):
+    torch = pytest.importorskip("torch")
+    from scrs_b200.serving import Server
+
+    reqs = [r for r in make_requests(torch, oracle, seed=5) if r[1] in (Engine.GOOD_CAUCHY, Engine.STANDARD_CAUCHY,
+                                                                        Engine.TOWER)]
+    biggest = max(r[2] * r[4] + (r[3] if r[0] == OP_ENCODE else r[2]) * r[4] for r in reqs)
+    srv = Server(gpu.lib, 3 * biggest, slots=8)  # a few requests' worth of memory
+    outs = run(srv, torch, reqs, list(range(len(reqs))))
+    for o, r in zip(outs, reqs):
+        assert np.array_equal(o.cpu().numpy(), r[-1])
+    srv.close()
+
+
+def test_submit_errors(gpu):
+    torch = pytest.importorskip("torch")
+    from scrs_b200.serving import Server
+
+    srv = Server(gpu.lib, 1 << 20, slots=2)
+    buf = torch.zeros(1 << 21, dtype=torch.uint8, device="cuda")
+    p = buf.data_ptr()
+    with pytest.raises(RuntimeFailure):  # 2 MiB request under a 1 MiB budget
+        srv.submit(OP_ENCODE, Engine.GOOD_CAUCHY, 16, 16, 65536, p, p)
+    with pytest.raises(ConfigError):
+        srv.submit(OP_ENCODE, Engine.GOOD_CAUCHY, 0, 4, 64, p, p)
+    with pytest.raises(DecodeError):  # duplicate index
+        srv.submit(OP_DECODE, Engine.GOOD_CAUCHY, 3, 2, 64, p, p, [0, 0, 1])
+    with pytest.raises(DecodeError):  # index out of range
+        srv.submit(OP_DECODE, Engine.GOOD_CAUCHY, 3, 2, 64, p, p, [0, 1, 9])
+    assert srv.pending == 0
+    srv.close()
