@@ -136,14 +136,9 @@ def dist_setup():
 
 
 def barrier_max(value: float, world: int) -> float:
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
+    from scrs_b200.shard import max_over_ranks
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return value if world == 1 else max_over_ranks(value)
 
 
 def barrier(world):
