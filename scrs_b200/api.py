@@ -438,8 +438,11 @@ class BatchDecoder(_Handle):
             indices, rows = symbols
             if scratch is None:
                 scratch = self.scratch()
-            n = len(indices)
-            idx = (C.c_uint64 * max(n, 1))(*[int(i) for i in indices])
+            ia = np.ascontiguousarray(np.asarray(indices, dtype=np.uint64).reshape(-1))
+            n = int(ia.size)
+            if n == 0:
+                ia = np.zeros(1, np.uint64)
+            idx = ia.ctypes.data_as(C.POINTER(C.c_uint64))
             rp, _ = _device_view(rows)
             op, ol = _device_view(out)
             st = self._lib.batch_decode_into_with_device(self._ptr, idx, rp, n, op, ol, scratch._ptr,

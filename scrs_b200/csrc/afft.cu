@@ -487,7 +487,7 @@ int32_t AfftCodec::init(uint64_t k_, uint64_t m_, uint64_t L_, scrs_error* err) 
     int32_t r = afft_locator_device(known.as<uint8_t>(), (uint32_t)ts, wa.as<uint32_t>(), wb.as<uint32_t>(),
                                     enc_values.as<uint16_t>(), enc_derivs.as<uint16_t>(), 0, err);
     if (r) return r;
-    SCRS_CUDA(cudaDeviceSynchronize());
+    SCRS_CUDA(cudaStreamSynchronize(0));  // the locator ran on the legacy stream
     return SCRS_OK;
 }
 

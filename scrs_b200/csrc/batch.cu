@@ -142,7 +142,7 @@ extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe
     if (items > b->max_items || items > 0xFFFFFFFFull) return set_err(err, SCRS_ERR_CAPACITY, items, b->max_items);
     const size_t arena_bytes = coef_bytes + slot_bytes;
     b->arena.assign(arena_bytes + 16, 0);
-    SCRS_CUDA(b->d_arena.ensure(b->arena.size()));
+    SCRS_CUDA(b->d_arena.ensure_grow(b->arena.size()));
     uint8_t* dbase = b->d_arena.as<uint8_t>();
     for (auto& kv : coef_off)
         hf::gf8_coefficients(std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first),
@@ -229,7 +229,7 @@ extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe
     for (size_t t = 0; t < b->tasks.size(); t++)
         std::fill(b->item_task.begin() + b->tasks[t].item_begin,
                   b->item_task.begin() + b->tasks[t].item_begin + b->tasks[t].n_items, (uint32_t)t);
-    SCRS_CUDA(b->d_item_task.ensure((size_t)item * 4));
+    SCRS_CUDA(b->d_item_task.ensure_grow((size_t)item * 4));
     if (item)
         SCRS_CUDA(cudaMemcpy(b->d_item_task.p, b->item_task.data(), (size_t)item * 4, cudaMemcpyHostToDevice));
     b->max_plan_r = max_r;

@@ -29,9 +29,9 @@ namespace {
 // Shared-memory header: mbarrier (0), item words (8, 12), task descriptor
 // (16), one step list per warp (kStepOffset).
 constexpr int kStepOffset = 128;
-constexpr int kStepBytes = 48;  // 2 * kSeg steps + fold marker + 1 read-ahead
+constexpr int kStepBytes = 144;  // u16 steps: 4 * kSeg + fold marker + 1 read-ahead
 constexpr int kSmemHeader = kStepOffset + 4 * kStepBytes;
-static_assert(2 * FieldGeom<0>::kSeg + 2 <= kStepBytes, "step list too short");
+static_assert(2 * (4 * FieldGeom<1>::kSeg + 2) <= kStepBytes, "step list too short");
 static_assert(FieldGeom<0>::kSeg <= 32 && FieldGeom<1>::kSeg <= 32, "one lane per staged row");
 constexpr uint32_t kTaskWords = (sizeof(MxkTask) + 3) / 4;
 static_assert(kTaskWords <= 32, "task descriptor must fit one warp's loads");
@@ -191,81 +191,81 @@ __device__ __forceinline__ void load_out_planes(const uint8_t* orow, uint64_t of
 // rows x_i, plus the row's existing content when `existing` (accumulate mode or
 // the partial sum of earlier segments).  `c` is lane i's coefficient c_i.
 //
-// GF(256): Horner on nibbles, c*x = 16*(hi*x) + lo*x, so the whole sum is
-// 16 * (XOR_i hi_i x_i) + XOR_i lo_i x_i and one 16-way table (v*x for v < 16,
-// the cheapest half of the multiplication table) serves both passes from a
-// single jump site.  The small table stays in the SM's instruction cache; a
+// Horner on nibbles.  GF(256): c*x = 16*(hi*x) + lo*x, so the whole sum is
+// 16 * (XOR_i hi_i x_i) + XOR_i lo_i x_i.  GF((2^8)^2), c = c0 + c1*u with
+// GF(256) components: c*x = c0*x + c1*(u*x), so the sum is
+// 16 * XOR_i (hi(c0_i) x_i + hi(c1_i) u x_i) + XOR_i (lo(c0_i) x_i + lo(c1_i) u x_i)
+// (a GF(256) scalar multiplies both tower components alike, and u*x is a
+// fixed XOR network computed on the fly).  Either way one 16-way table
+// (v*x for v < 16, the cheapest half of the multiplication table) serves every
+// step from a single jump site, so it stays in the SM's instruction cache; a
 // 256-way or two 16-way tables do not, and their misses cost more than the
-// second pass over the staged rows.  The warp runs a step list: (i << 4) | hi_i
-// for the nonzero high nibbles, a fold marker 0, then (i << 4) | lo_i.
+// second pass over the staged rows.  The warp runs a step list of
+// (i << 5) | (u-flag << 4) | nibble entries: the high-nibble pass, a fold
+// marker 0, then the low-nibble pass.
 template <int kGf16>
-__device__ __forceinline__ void output_row(const uint8_t* buf, uint32_t c, uint8_t* steps, uint32_t seg_n, int lane,
+__device__ __forceinline__ void output_row(const uint8_t* buf, uint32_t c, uint16_t* steps, uint32_t seg_n, int lane,
                                            bool existing, uint8_t* orow, uint64_t off, uint64_t L, bool aligned,
                                            bool full) {
     using G = FieldGeom<kGf16>;
     using Words = typename Lane<kGf16>::Words;
     constexpr int kWords = Lane<kGf16>::kWords;
+    static_assert(kWords == 16, "one 16-plane set per lane");
     Words acc;
-    if constexpr (kGf16) {
-        if (existing) {
-            load_out_planes<kGf16>(orow, off, lane, L, aligned, acc);
-        } else {
+    // nibbles of the x-term (c0, or the GF(256) coefficient) and the u-term (c1)
+    const uint32_t cx = c & 0xFFu, cu = kGf16 ? (c >> 8) & 0xFFu : 0u;
+    const uint32_t below = (1u << lane) - 1u;
+    uint32_t n_steps = 0;
 #pragma unroll
-            for (int t = 0; t < kWords; t++) acc[t] = 0;
+    for (int pass = 0; pass < 2; pass++) {
+        const uint32_t vx = pass ? cx & 15u : cx >> 4, vu = pass ? cu & 15u : cu >> 4;
+        const uint32_t mx = __ballot_sync(0xFFFFFFFFu, vx != 0), mu = __ballot_sync(0xFFFFFFFFu, vu != 0);
+        const uint32_t at = n_steps + __popc(mx & below) + __popc(mu & below);
+        if (vx) steps[at] = (uint16_t)((lane << 5) | vx);
+        if (vu) steps[at + (vx != 0)] = (uint16_t)((lane << 5) | 16u | vu);
+        n_steps += __popc(mx) + __popc(mu);
+        if (pass == 0) {
+            if (lane == 0) steps[n_steps] = 0;  // fold marker
+            n_steps++;
         }
-        for (uint32_t i = 0; i < seg_n; i++) {
-            const uint32_t ci = __shfl_sync(0xFFFFFFFFu, c, i);
-            if (ci == 0) continue;
-            Words p;
-            load_lane<kGf16>(buf + (size_t)i * G::kChunk, lane, p);
-            mul_planes<kGf16>(ci, acc, p);
-        }
-    } else {
-        const uint32_t hi = c >> 4, lo = c & 15u;
-        const uint32_t mh = __ballot_sync(0xFFFFFFFFu, hi != 0), ml = __ballot_sync(0xFFFFFFFFu, lo != 0);
-        const uint32_t below = (1u << lane) - 1u;
-        const uint32_t nh = __popc(mh);
-        if (hi) steps[__popc(mh & below)] = (uint8_t)((lane << 4) | hi);
-        if (lo) steps[nh + 1 + __popc(ml & below)] = (uint8_t)((lane << 4) | lo);
-        if (lane == 0) steps[nh] = 0;
-        __syncwarp();
-        const uint32_t n_steps = nh + 1 + __popc(ml);
-#pragma unroll
-        for (int t = 0; t < kWords; t++) acc[t] = 0;
-        const uint8_t* lane_buf = buf + 16 * lane;
-        uint32_t d = steps[0];
-        for (uint32_t s = 0; s < n_steps; s++) {
-            const uint32_t dn = steps[s + 1];
-            if (d == 0) {  // high nibbles done: acc = 16 * acc, plus the existing content
-#pragma unroll
-                for (int h = 0; h < kWords; h += 8) {
-                    uint32_t t16[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-                    mulacc8<16>(t16, *reinterpret_cast<const uint32_t(*)[8]>(&acc[h]));
-#pragma unroll
-                    for (int r = 0; r < 8; r++) acc[h + r] = t16[r];
-                }
-                if (existing) {
-                    Words e;
-                    load_out_planes<kGf16>(orow, off, lane, L, aligned, e);
-#pragma unroll
-                    for (int t = 0; t < kWords; t++) acc[t] ^= e[t];
-                }
-            } else {
-                Words p;
-                const uint8_t* src = lane_buf + (d >> 4) * (uint32_t)G::kChunk;
-#pragma unroll
-                for (int pc = 0; pc < 4; pc++) {
-                    const uint4 v = *reinterpret_cast<const uint4*>(src + pc * 512);
-                    p[4 * pc] = v.x, p[4 * pc + 1] = v.y, p[4 * pc + 2] = v.z, p[4 * pc + 3] = v.w;
-                }
-#if defined(__CUDA_ARCH__)
-                brx_mul8x2_lo(d & 15u, acc, p);
-#endif
-            }
-            d = dn;
-        }
-        __syncwarp();  // the list is rebuilt for the warp's next output row
     }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < kWords; t++) acc[t] = 0;
+    const uint8_t* lane_buf = buf + 16 * lane;
+    uint32_t d = steps[0];
+    for (uint32_t s = 0; s < n_steps; s++) {
+        const uint32_t dn = steps[s + 1];
+        if (d == 0) {  // high nibbles done: acc = 16 * acc, plus the existing content
+#pragma unroll
+            for (int h = 0; h < kWords; h += 8) {
+                uint32_t t16[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                mulacc8<16>(t16, *reinterpret_cast<const uint32_t(*)[8]>(&acc[h]));
+#pragma unroll
+                for (int r = 0; r < 8; r++) acc[h + r] = t16[r];
+            }
+            if (existing) {
+                Words e;
+                load_out_planes<kGf16>(orow, off, lane, L, aligned, e);
+#pragma unroll
+                for (int t = 0; t < kWords; t++) acc[t] ^= e[t];
+            }
+        } else {
+            Words p;
+            const uint8_t* src = lane_buf + (d >> 5) * (uint32_t)G::kChunk;
+#pragma unroll
+            for (int pc = 0; pc < 4; pc++) {
+                const uint4 v = *reinterpret_cast<const uint4*>(src + pc * 512);
+                p[4 * pc] = v.x, p[4 * pc + 1] = v.y, p[4 * pc + 2] = v.z, p[4 * pc + 3] = v.w;
+            }
+            if (kGf16 && (d & 16u)) mul_by_u(p);
+#if defined(__CUDA_ARCH__)
+            brx_mul8x2_lo(d & 15u, acc, p);
+#endif
+        }
+        d = dn;
+    }
+    __syncwarp();  // the list is rebuilt for the warp's next output row
     bitslice_lane<kGf16>(acc);
     store_pieces<Lane<kGf16>::kPieces>(orow, off, 0, lane, L, aligned, full, acc);
 }
@@ -289,7 +289,7 @@ __device__ bool process_item(const MxkTask& T, uint32_t chunk, uint8_t* buf, uin
     const uint32_t n_in = T.n_in;
     const bool aligned = T.aligned != 0;
     const bool full = aligned && off + G::kChunk <= L;
-    uint8_t* steps = steps_base + warp * kStepBytes;
+    uint16_t* steps = reinterpret_cast<uint16_t*>(steps_base + warp * kStepBytes);
 
     for (uint32_t og = out_lo; og == out_lo || og < out_hi; og += kMaxOutGroup) {
         const uint32_t og_n = out_hi > og ? umin32(kMaxOutGroup, out_hi - og) : 0;
@@ -707,11 +707,13 @@ cudaError_t launch_single_impl(const MxkTask& T, int32_t* status, int grid, cuda
     cudaError_t e = set_mxk_attrs<kGf16>();
     if (e != cudaSuccess) return e;
     int seg_cap = std::max(1, std::min((int)T.n_in, G::kSeg));
-    // Split the outputs when the row chunks alone cannot fill the GPU.
+    // Split the outputs when the row chunks alone cannot fill the GPU, keeping
+    // at least one output per warp in each split (every split re-stages and
+    // re-slices the chunk's input rows).
     constexpr uint32_t kTargetItems = 2 * 148;
     uint32_t per = std::max<uint32_t>(T.n_out, 1);
-    if (T.n_items < kTargetItems && T.n_out > 1) {
-        uint32_t splits = std::min<uint32_t>(T.n_out, (kTargetItems + T.n_items - 1) / T.n_items);
+    if (T.n_items < kTargetItems && T.n_out > 4) {
+        const uint32_t splits = std::min<uint32_t>((T.n_out + 3) / 4, (kTargetItems + T.n_items - 1) / T.n_items);
         per = (T.n_out + splits - 1) / splits;
     }
     const uint32_t items = T.n_items * (T.n_out ? (T.n_out + per - 1) / per : 1);

@@ -53,6 +53,13 @@ struct DevBuf {
         else p = nullptr;
         return e;
     }
+    // As ensure(), but a reallocation takes twice the current size when that
+    // is larger, so a buffer that grows in small steps reallocates (and
+    // synchronises the device in cudaFree) only a logarithmic number of times.
+    cudaError_t ensure_grow(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        return ensure(n > 2 * bytes ? n : 2 * bytes);
+    }
     template <class T>
     T* as() const { return reinterpret_cast<T*>(p); }
 };

@@ -268,16 +268,31 @@ void retire(scrs_server* s, Slot& sl, uint64_t t_done) {
     sl.busy = false;
 }
 
-// Admit waiting requests into idle slots (first come, first served).
+// Admit waiting requests into idle slots (first come, first served).  A tower
+// or AFFT request goes to an idle slot that already holds its profile's
+// engines when there is one (building engines allocates device memory).
 void admit(scrs_server* s) {
-    for (auto& slp : s->slots) {
-        Slot& sl = *slp;
-        if (sl.busy || s->queue.empty()) continue;
+    for (;;) {
+        if (s->queue.empty()) return;
         Req& head = s->queue.front();
         if (s->in_use + head.bytes > s->budget) return;  // wait for memory
+        Slot* pick = nullptr;
+        const bool gf256 = is_gf256(head.d.engine);
+        for (auto& slp : s->slots) {
+            if (slp->busy) continue;
+            if (!pick) pick = slp.get();
+            if (gf256) break;
+            const ProfileKey key{head.d.engine, head.d.k, head.d.m, head.d.symbol_len};
+            if (slp->cache.count(key)) {
+                pick = slp.get();
+                break;
+            }
+        }
+        if (!pick) return;  // every slot busy
+        Slot& sl = *pick;
         std::vector<Req> group;
         uint64_t held = 0;
-        if (is_gf256(head.d.engine)) {
+        if (gf256) {
             // coalesce every waiting GF(256) request that fits, in arrival order
             for (auto it = s->queue.begin(); it != s->queue.end() && group.size() < kMaxCoalesce;) {
                 if (!is_gf256(it->d.engine)) {
@@ -299,7 +314,7 @@ void admit(scrs_server* s) {
         sl.busy = true;
         sl.running = std::move(group);
         int32_t rc;
-        if (is_gf256(sl.running[0].d.engine)) {
+        if (gf256) {
             rc = launch_group(sl, sl.running, &sl.launch_err);
             s->stats.batches++;
         } else {

@@ -309,3 +309,47 @@ def test_stripe_batch_matches_oracle(gpu, oracle):
         for o, exp in zip(outs, expect):
             assert np.array_equal(o.cpu().numpy(), exp), mode
     assert b.last_launches == 2  # plan + persistent drain
+
+
+def test_stripe_batch_host_buffers_pipelined(gpu, oracle):
+    """Host-buffer batches run in up to 16 pieces whose copies overlap the
+    compute; results must equal the oracle's, run after run."""
+    torch = pytest.importorskip("torch")
+    from scrs_b200.batch import OP_DECODE, OP_ENCODE, StripeBatch
+
+    specs, rng = make_mixed_batch(torch, 40, 9, lens=(1024, 4096, 1000, 64), kmax=24, mmax=8)
+    n = len(specs)
+    ops, engines, ks, ms, Ls, ins, outs, expect, keep = [], [], [], [], [], [], [], [], []
+    kmax = max(s[2] for s in specs)
+    indices = np.zeros((n, kmax), np.uint16)
+    for s, (op, engine, k, m, L) in enumerate(specs):
+        p = oracle.resolve(engine, k, m, L)
+        data = rng.integers(0, 256, k * L, dtype=np.uint8)
+        if op == OP_ENCODE:
+            exp = np.zeros(m * L, np.uint8)
+            oracle.batch_encoder(p).encode_into(data, exp)
+            h_in = torch.from_numpy(data).pin_memory()
+        else:
+            word = encode_word(oracle, p, data)
+            e = int(rng.integers(0, min(k, m) + 1))
+            erased = rng.choice(k, e, replace=False).tolist()
+            idx = [i for i in range(k) if i not in erased] + [k + j for j in rng.choice(m, e, replace=False).tolist()]
+            idx = rng.permutation(idx).tolist()
+            indices[s, :k] = idx
+            h_in = torch.from_numpy(np.concatenate([word[i] for i in idx])).pin_memory()
+            exp = data
+        h_out = torch.zeros(len(exp), dtype=torch.uint8).pin_memory()
+        ops.append(op), engines.append(int(engine)), ks.append(k), ms.append(m), Ls.append(L)
+        ins.append(h_in.data_ptr()), outs.append(h_out.data_ptr())
+        expect.append(exp), keep.append((h_in, h_out))
+    b = StripeBatch(gpu.lib, n)
+    b.set_arrays(np.array(ops), np.array(engines), np.array(ks), np.array(ms), np.array(Ls),
+                 np.array(ins, dtype=np.uint64), np.array(outs, dtype=np.uint64), indices=indices, host=True)
+    for _ in range(2):
+        for _, h_out in keep:
+            h_out.zero_()
+        b.run()
+        torch.cuda.synchronize()
+        b.check()
+        for (_, h_out), exp in zip(keep, expect):
+            assert np.array_equal(h_out.numpy(), exp)
