@@ -378,7 +378,7 @@ def extra_latency(torch, api):
         res[f"{name}_p50_ms"] = round(float(np.percentile(ts, 50)), 4)
         res[f"{name}_p99_ms"] = round(float(np.percentile(ts, 99)), 4)
     assert torch.equal(out, data)
-    res["workload"] = "one stripe k=10 m=4 L=4096, device buffers, per-call launch (encode: 1 kernel; decode: plan+1)"
+    res["workload"] = "one stripe k=10 m=4 L=4096, device buffers, per-call launch (encode: 1 kernel; decode: 1 kernel, the plan comes from the recipe cache after the first call)"
     return res
 
 

@@ -209,6 +209,15 @@ SCRS_API int32_t scrs_batch_decode_into_with_device(scrs_batch_decoder* dec,
                                            scrs_batch_decode_scratch* scratch,
                                            void* stream, scrs_error* err);
 
+/* Decode recipes (the reduced inverse's coefficients) are kept in a small
+ * device-resident LRU per decode scratch, keyed by the erasure pattern, as
+ * the reference's RecipeCache (decoder/cache.rs:15-100): a repeated pattern
+ * skips the plan launch.  Returns how many decodes hit it.  A scratch's
+ * device work must stay ordered on one stream (the reference's scratch is
+ * exclusively borrowed). */
+SCRS_API uint64_t scrs_batch_decode_scratch_recipe_hits(const scrs_batch_decode_scratch* scratch);
+SCRS_API uint64_t scrs_decode_scratch_recipe_hits(const scrs_decode_scratch* scratch);
+
 /* GF(256) batch decode that allocates nothing (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc: the allocation may
  * synchronise the device, which a latency-bound receive loop cannot afford,

@@ -206,6 +206,8 @@ _DEVICE_SIGNATURES = [
     ("dec_push_device", _I32, [_P, _U64, _BUF, _U64, C.POINTER(_Push), C.POINTER(_Error)]),
     ("dec_finalize_into_with_device", _I32, [_P, _BUF, _U64, _P, _P, C.POINTER(_Error)]),
     ("status_name", C.c_char_p, [_I32]),
+    ("batch_decode_scratch_recipe_hits", _U64, [_P]),
+    ("decode_scratch_recipe_hits", _U64, [_P]),
 ]
 
 
@@ -354,9 +356,19 @@ class EncodeScratch(_Handle):
 class BatchDecodeScratch(_Handle):
     _destroy = "batch_decode_scratch_destroy"
 
+    @property
+    def recipe_hits(self) -> int:
+        """Decodes whose erasure pattern was found in the device recipe cache."""
+        return int(self._lib.batch_decode_scratch_recipe_hits(self._ptr))
+
 
 class DecodeScratch(_Handle):
     _destroy = "decode_scratch_destroy"
+
+    @property
+    def recipe_hits(self) -> int:
+        """Finalizes whose erasure pattern was found in the device recipe cache."""
+        return int(self._lib.decode_scratch_recipe_hits(self._ptr))
 
 
 class BatchEncoder(_Handle):

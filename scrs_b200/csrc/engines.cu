@@ -53,20 +53,68 @@ struct TowerTables {
 
 // Reduced-solve recipe buffers: lists for the plan kernel and the
 // multiply-XOR task, plus the coefficient rows (received repairs first,
-// then present data).
+// then present data).  Coefficients are kept in a small device-resident LRU
+// keyed by the erasure pattern (missing data indices + the repair columns
+// used), as the reference's RecipeCache (decoder/cache.rs:15-100) keeps
+// recipes: a repeated pattern skips the plan launch.
 struct RecipeBufs {
+    struct Entry {
+        std::vector<uint16_t> key;  // r, missing[r], repairs[r]
+        DevBuf coef;                // elem[k * r]
+        uint64_t last_use = 0;
+    };
+    static constexpr size_t kCacheEntries = 32;
     DevBuf lists;   // uint16: in_rows[k] pass_rows[k] out_rows[rmax] missing[rmax] repairs[rmax] present[k]
-    DevBuf coef;    // elem[k * rmax]
     DevBuf work;    // uint32[4*rmax] when rmax exceeds the shared-memory plan limit
     std::vector<uint16_t> host;  // same layout as `lists`
+    std::vector<std::unique_ptr<Entry>> cache;
+    uint64_t clock = 0, hits = 0;
     uint32_t k = 0, rmax = 0, elem = 1;
     cudaError_t init(uint32_t k_, uint32_t rmax_, uint32_t elem_) {
         k = k_, rmax = rmax_, elem = elem_;
         host.assign((size_t)3 * k + 3 * rmax + 8, 0);
         cudaError_t e = lists.ensure(host.size() * sizeof(uint16_t));
-        if (e == cudaSuccess) e = coef.ensure((size_t)k * std::max<uint32_t>(rmax, 1) * elem);
         if (e == cudaSuccess && rmax > kPlanSmemMaxR) e = work.ensure((size_t)4 * rmax * sizeof(uint32_t));
         return e;
+    }
+    // Coefficient buffer for the pattern; *fresh says whether it must be
+    // (re)computed.  The least recently used entry is reused when full.
+    cudaError_t lookup(const std::vector<uint16_t>& missing, const std::vector<uint16_t>& repairs, void** coef,
+                       bool* fresh) {
+        std::vector<uint16_t> key;
+        key.reserve(1 + missing.size() + repairs.size());
+        key.push_back((uint16_t)missing.size());
+        key.insert(key.end(), missing.begin(), missing.end());
+        key.insert(key.end(), repairs.begin(), repairs.end());
+        for (auto& e : cache)
+            if (e->key == key) {
+                e->last_use = ++clock;
+                hits++;
+                *coef = e->coef.p;
+                *fresh = false;
+                return cudaSuccess;
+            }
+        Entry* slot = nullptr;
+        if (cache.size() < kCacheEntries) {
+            cache.emplace_back(new Entry());
+            slot = cache.back().get();
+        } else {
+            slot = cache[0].get();
+            for (auto& e : cache)
+                if (e->last_use < slot->last_use) slot = e.get();
+        }
+        // Reusing a buffer that a queued kernel may still read is safe: its
+        // pattern's plan and multiply ran earlier on the same stream.
+        cudaError_t e = slot->coef.ensure((size_t)k * std::max<size_t>(missing.size(), 1) * elem);
+        if (e != cudaSuccess) {
+            slot->key.clear();
+            return e;
+        }
+        slot->key = std::move(key);
+        slot->last_use = ++clock;
+        *coef = slot->coef.p;
+        *fresh = true;
+        return cudaSuccess;
     }
     uint16_t* h_in() { return host.data(); }
     uint16_t* h_pass() { return host.data() + k; }
@@ -107,7 +155,10 @@ int32_t run_cauchy_recover(RecipeBufs& rb, int32_t engine, uint32_t k, const std
     SCRS_CUDA(cudaMemcpyAsync(rb.lists.p, rb.host.data(), rb.host.size() * sizeof(uint16_t),
                               cudaMemcpyHostToDevice, s));
     const uint32_t K = rb.k, R = rb.rmax;
-    if (r) {
+    void* coef = nullptr;
+    bool fresh = true;
+    if (r) SCRS_CUDA(rb.lookup(missing, repairs, &coef, &fresh));
+    if (r && fresh) {
         CauchyPlanTask P{};
         P.r = r;
         P.p = p;
@@ -118,14 +169,14 @@ int32_t run_cauchy_recover(RecipeBufs& rb, int32_t engine, uint32_t k, const std
         P.repairs = rb.d(2 * K + 2 * R);
         P.present = rb.d(2 * K + 3 * R);
         P.powers = d_powers;
-        P.coef = rb.coef.p;
+        P.coef = coef;
         P.work = r > kPlanSmemMaxR ? rb.work.as<uint32_t>() : nullptr;
         SCRS_CUDA(launch_cauchy_plan_single(P, gf16 ? 1 : 0, s));
     }
     MxkTask T{};
     T.in = src;
     T.out = out;
-    T.coef = rb.coef.p;
+    T.coef = coef;
     T.in_rows = rb.d(0);
     T.out_rows = rb.d(2 * K);
     T.pass_rows = rb.d(K);
@@ -1030,6 +1081,15 @@ extern "C" void scrs_inc_reset(scrs_incremental_encoder* e) {
     std::fill(e->pending_dev.begin(), e->pending_dev.end(), 0);
     e->pending.clear();
     e->fed_count = 0;
+}
+
+// Recipe-cache hits (repeated erasure patterns that skipped the plan launch).
+extern "C" uint64_t scrs_decode_scratch_recipe_hits(const scrs_decode_scratch* s) {
+    return s ? s->recipe.hits : 0;
+}
+extern "C" uint64_t scrs_batch_decode_scratch_recipe_hits(const scrs_batch_decode_scratch* s) {
+    if (!s) return 0;
+    return s->lazy ? s->lazy->recipe.hits : s->recipe.hits;
 }
 
 // Device-side status of a handle's last asynchronous work (used by the

@@ -353,3 +353,33 @@ def test_stripe_batch_host_buffers_pipelined(gpu, oracle):
         b.check()
         for (_, h_out), exp in zip(keep, expect):
             assert np.array_equal(h_out.numpy(), exp)
+
+
+@pytest.mark.parametrize("engine,k,m,L", [(Engine.GOOD_CAUCHY, 10, 4, 4096), (Engine.STANDARD_CAUCHY, 6, 3, 100),
+                                          (Engine.TOWER, 8, 4, 1024)])
+def test_recipe_cache_repeated_patterns(gpu, oracle, engine, k, m, L):
+    """Repeated erasure patterns reuse the device-resident recipe (LRU of 32);
+    every decode stays exact through hits, misses and evictions."""
+    p = gpu.resolve(engine, k, m, L)
+    data = gfpy.rng_bytes(k * L, 77)
+    word = encode_word(oracle, p, data)
+    pats = [s for s in k_subsets(k + m, k) if any(i >= k for i in s)][:40]
+    assert len(pats) == 40
+    dec = gpu.batch_decoder(p)
+    s = dec.scratch()
+    seq = pats + [pats[39], pats[10], pats[0]]
+    for q, sub in enumerate(seq):
+        out = np.full(k * L, 0xAB, np.uint8)
+        dec.decode_into_with([(i, word[i]) for i in sub], out, s)
+        assert np.array_equal(out, data), q
+    assert s.recipe_hits == 2  # pats[39] and pats[10]; pats[0] was evicted
+    lazy = gpu.decoder(p)
+    ls = lazy.scratch()
+    for sub in (pats[5], pats[5], pats[6], pats[5]):
+        lazy.reset()
+        for i in sub:
+            lazy.push(i, word[i])
+        out = np.zeros(k * L, np.uint8)
+        lazy.finalize_into_with(out, ls)
+        assert np.array_equal(out, data)
+    assert ls.recipe_hits == 2
