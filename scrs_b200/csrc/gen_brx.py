@@ -32,20 +32,61 @@ def rows_of(c):
     return [[s for s in range(8) if (cols[s] >> r) & 1] for r in range(8)]
 
 
+def cse_rows(rows):
+    """Greedy common-subexpression pass: while some pair of planes occurs in two
+    or more rows and sharing it lowers the instruction count, XOR the pair once
+    into a temporary and use that in those rows.  Returns (pairs, rows) with
+    temporaries numbered 8, 9, ... after the 8 planes."""
+    def cost(rs):
+        return sum((len(t) + 1) // 2 for t in rs)
+
+    rows = [list(r) for r in rows]
+    pairs = []
+    while True:
+        count = {}
+        for r in rows:
+            rr = sorted(r)
+            for i in range(len(rr)):
+                for j in range(i + 1, len(rr)):
+                    count[(rr[i], rr[j])] = count.get((rr[i], rr[j]), 0) + 1
+        best = None
+        for (a, b), n in sorted(count.items()):
+            if n < 2:
+                continue
+            t = 8 + len(pairs)
+            new = [[x for x in r if x not in (a, b)] + [t] if (a in r and b in r) else r for r in rows]
+            gain = cost(rows) - cost(new) - 1
+            if gain > 0 and (best is None or gain > best[0]):
+                best = (gain, (a, b), new)
+        if best is None:
+            return pairs, rows
+        pairs.append(best[1])
+        rows = best[2]
+
+
+MAX_TEMPS = 8
+
+
 def case_body(c, acc_base, p_base, halves, prefix):
-    """PTX lines applying coefficient c to `halves` groups of 8 planes: each
-    output plane takes its terms two at a time with a 3-input XOR (lop3 0x96)."""
+    """PTX lines applying coefficient c to `halves` groups of 8 planes: shared
+    plane pairs are XORed once into temporaries, then each output plane takes
+    its terms two at a time with a 3-input XOR (lop3 0x96)."""
     lines = []
-    rows = rows_of(c)
+    pairs, rows = cse_rows(rows_of(c))
+    assert len(pairs) <= MAX_TEMPS
     for h in range(halves):
+        def op(t):
+            return f"%{p_base + 8 * h + t}" if t < 8 else f"cse{t - 8}"
+        for i, (a, b) in enumerate(pairs):
+            lines.append(f"xor.b32 cse{i}, {op(a)}, {op(b)};")
         for r in range(8):
-            a = acc_base + 8 * h + r
-            terms = [p_base + 8 * h + s for s in rows[r]]
+            a = f"%{acc_base + 8 * h + r}"
+            terms = list(rows[r])
             while len(terms) >= 2:
                 x, y = terms.pop(0), terms.pop(0)
-                lines.append(f"lop3.b32 %{a}, %{a}, %{x}, %{y}, 0x96;")
+                lines.append(f"lop3.b32 {a}, {a}, {op(x)}, {op(y)}, 0x96;")
             if terms:
-                lines.append(f"xor.b32 %{a}, %{a}, %{terms[0]};")
+                lines.append(f"xor.b32 {a}, {a}, {op(terms[0])};")
     return lines
 
 
@@ -71,7 +112,7 @@ def asm_function(fname, doc, nplanes, blocks, uniform=True):
     p_ops = ", ".join(f'"r"(p[{i}])' for i in range(nplanes))
     idx_names = [b[1] for b in blocks]
     idx_ops = ", ".join(f'"r"({n})' for n in idx_names)
-    body = ["{"]
+    body = ["{", f".reg .b32 cse<{MAX_TEMPS}>;"]
     for bi, (coeffs, _) in enumerate(blocks):
         idx_operand = 2 * nplanes + bi
         body += dispatch(fname, coeffs, halves, 0, nplanes, idx_operand, f"L{fname[:2]}{bi}_", f"L{fname[:2]}{bi}_D",
