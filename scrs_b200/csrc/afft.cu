@@ -312,13 +312,15 @@ __global__ void __launch_bounds__(kPassThreads) afft_pass_kernel(uint8_t* work, 
     const uint32_t g0 = ct * gt;
     const uint32_t gn = min(gt, G - g0);
     auto row_of = [&](uint32_t i) { return (hi << (D - l0)) | (i << low_bits) | lo; };
-    // load: element (i, g, q) = 16 bytes, smem at ((i*4 + q)*gt + g)*16
+    // load: element (i, g, q) = 16 bytes, smem at ((i*4 + q)*gt + g)*16; the
+    // copies are asynchronous, so every thread has all of its loads in flight
     const uint32_t pieces = rows_in_tile * gn * 4;
     for (uint32_t x = tid; x < pieces; x += blockDim.x) {
         const uint32_t q = x & 3, g = (x >> 2) % gn, i = (x >> 2) / gn;
-        const uint4 v = *reinterpret_cast<const uint4*>(work + ((uint64_t)row_of(i) * G + g0 + g) * 64 + 16 * q);
-        *reinterpret_cast<uint4*>(tile + ((size_t)(i * 4 + q) * gt + g) * 16) = v;
+        cp_async_16(tile + ((size_t)(i * 4 + q) * gt + g) * 16,
+                    work + ((uint64_t)row_of(i) * G + g0 + g) * 64 + 16 * q);
     }
+    cp_async_wait_all();
     __syncthreads();
     const uint32_t pairs = rows_in_tile / 2;
     for (int s = 0; s < c; s++) {
@@ -420,11 +422,15 @@ cudaError_t run_wht(uint32_t* v, uint32_t ts, int D, cudaStream_t st) {
         if (e != cudaSuccess) return e;
         attr = true;
     }
+    // passes of at most 8 index bits: enough groups per pass to spread over
+    // the SMs (one CTA per group of 2^nb elements)
     std::vector<std::pair<int, int>> passes;
-    if (D <= 13)
-        passes.push_back({0, D});
-    else
-        passes = {{0, 8}, {8, D - 8}};
+    const int n_pass = (D + 7) / 8;
+    for (int q = 0, lo = 0; q < n_pass; q++) {
+        const int nb = (D - lo + (n_pass - q) - 1) / (n_pass - q);
+        passes.push_back({lo, nb});
+        lo += nb;
+    }
     for (auto& p : passes) {
         uint32_t groups = ts >> p.second;
         uint32_t gsize = 1u << p.second;

@@ -155,6 +155,16 @@ __device__ __forceinline__ void tma_load_1d(void* smem_dst, const void* gmem_src
         : "memory");
 }
 
+// 16-byte asynchronous global -> shared copy (no register staging), so a
+// thread keeps many tile loads in flight; cp_async_wait_all() waits for this
+// thread's copies.
+__device__ __forceinline__ void cp_async_16(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(smem_dst)), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // Bulk prefetch of [src, src + bytes) into L2 (src 16-byte aligned, bytes a
 // multiple of 16).
 __device__ __forceinline__ void prefetch_l2_bulk(const void* gmem_src, uint32_t bytes) {
