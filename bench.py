@@ -424,10 +424,12 @@ def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C25
         op, engine, k, m, Ls, d_in, d_out, idx = templates[t]
         srv.submit(op, engine, k, m, Ls, d_in.data_ptr(), d_out.data_ptr(), idx, tag=tag)
 
-    # warm the resident engines, then the closed-loop capacity
-    for t in range(len(templates)):
-        submit(t, t)
-    srv.drain(600)
+    # warm the resident engines on every slot (building engines allocates device
+    # memory, a one-time cost per profile and slot), then the closed-loop capacity
+    for _ in range(8):
+        for t in range(len(templates)):
+            submit(t, t)
+        srv.drain(600)
     order = rng.integers(0, len(templates), 2000)
     t0 = time.perf_counter()
     for i, t in enumerate(order):
@@ -539,6 +541,10 @@ def extra_afft(torch, api):
     return res
 
 
+EXTRAS = {"batched_vs_plain_cfg4": extra_mixed, "latency_cfg1": extra_latency, "tower_cfg2": extra_tower,
+          "afft_cfg3": extra_afft, "serving_cfg5": extra_serving}
+
+
 # ---------------------------------------------------------------------------
 # arms
 # ---------------------------------------------------------------------------
@@ -631,8 +637,7 @@ def run_ours(args, world, rank, local):
         launches += hb.last_launches * n_e2e
     extras = {}
     if rank == 0 and not args.no_extras:
-        for name, fn in (("batched_vs_plain_cfg4", extra_mixed), ("latency_cfg1", extra_latency),
-                         ("tower_cfg2", extra_tower), ("afft_cfg3", extra_afft), ("serving_cfg5", extra_serving)):
+        for name, fn in EXTRAS.items():
             try:
                 extras[name] = fn(torch, api)
             except Exception as ex:  # reported, never hidden
@@ -696,8 +701,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg (profiling runs)")
     ap.add_argument("--stripes", type=int, default=STRIPES,
                     help="stripes per op per GPU; the headline uses 65536, smaller values are for ncu captures")
+    ap.add_argument("--only", choices=sorted(EXTRAS),
+                    help="run just one of the extras and print its JSON (profiling runs; no headline line)")
     args = ap.parse_args()
     STRIPES = args.stripes
+    if args.only:
+        import torch
+        import scrs_b200
+
+        print(json.dumps({args.only: EXTRAS[args.only](torch, scrs_b200.api_default())}))
+        return
     world, rank, local = dist_setup()
     try:
         if args.impl == "reference":

@@ -209,6 +209,13 @@ SCRS_API int32_t scrs_batch_decode_into_with_device(scrs_batch_decoder* dec,
                                            scrs_batch_decode_scratch* scratch,
                                            void* stream, scrs_error* err);
 
+/* Self-test of the device-side failure path (no reference counterpart):
+ * launches one bounded wait that nothing completes and returns the status it
+ * reports, SCRS_ERR_DEVICE_TIMEOUT after about limit_ns (1 ns .. 100 ms);
+ * the context stays usable.  Every wait in the kernels is bounded the same
+ * way (2 s) and reports through the same status word. */
+SCRS_API int32_t scrs_selftest_wait_timeout(uint64_t limit_ns, scrs_error* err);
+
 /* Decode recipes (the reduced inverse's coefficients) are kept in a small
  * device-resident LRU per decode scratch, keyed by the erasure pattern, as
  * the reference's RecipeCache (decoder/cache.rs:15-100): a repeated pattern

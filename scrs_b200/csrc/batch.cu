@@ -40,6 +40,7 @@ struct scrs_stripe_batch {
     uint64_t last_launches = 0;
     int sm_count = 0;
     std::vector<uint32_t> plan_begin;  // plans of stripes before stripe s
+    PinnedBuf upload;                  // staging of asynchronous set uploads
     // host-buffer mode
     struct Copy {
         const void* src;
@@ -96,8 +97,22 @@ extern "C" uint64_t scrs_stripe_batch_last_launches(const scrs_stripe_batch* b) 
     return b ? b->last_launches : 0;
 }
 
+namespace scrs {
+// set() with the uploads either synchronous (async_stream == false) or staged
+// through pinned memory and enqueued on `stream` (the serving loop's form:
+// no host wait; the batch must not be set again before that stream has run
+// the uploads).
+int32_t stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc* descs, uint64_t count, bool async_stream,
+                              cudaStream_t stream, scrs_error* err);
+}  // namespace scrs
+
 extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe_desc* descs, uint64_t count,
                                          scrs_error* err) {
+    return stripe_batch_set_impl(b, descs, count, false, nullptr, err);
+}
+
+int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc* descs, uint64_t count,
+                                    bool async_stream, cudaStream_t stream, scrs_error* err) {
     if (!b || (count && !descs)) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
     if (count > b->max_stripes) return set_err(err, SCRS_ERR_CAPACITY, count, b->max_stripes);
     // ---- validate and size the arena: [encode coefficient tables][decode slots]
@@ -230,16 +245,31 @@ extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe
         std::fill(b->item_task.begin() + b->tasks[t].item_begin,
                   b->item_task.begin() + b->tasks[t].item_begin + b->tasks[t].n_items, (uint32_t)t);
     SCRS_CUDA(b->d_item_task.ensure_grow((size_t)item * 4));
-    if (item)
-        SCRS_CUDA(cudaMemcpy(b->d_item_task.p, b->item_task.data(), (size_t)item * 4, cudaMemcpyHostToDevice));
     b->max_plan_r = max_r;
     if (off > arena_bytes) return set_err(err, SCRS_ERR_CAPACITY, off, arena_bytes);  // layout invariant
-    SCRS_CUDA(cudaMemcpy(b->d_arena.p, b->arena.data(), b->arena.size(), cudaMemcpyHostToDevice));
-    if (!b->tasks.empty())
-        SCRS_CUDA(cudaMemcpy(b->d_tasks.p, b->tasks.data(), b->tasks.size() * sizeof(MxkTask), cudaMemcpyHostToDevice));
-    if (!b->plans.empty())
-        SCRS_CUDA(cudaMemcpy(b->d_plans.p, b->plans.data(), b->plans.size() * sizeof(CauchyPlanTask),
-                             cudaMemcpyHostToDevice));
+    struct Up {
+        void* dst;
+        const void* src;
+        size_t bytes;
+    } ups[4] = {{b->d_item_task.p, b->item_task.data(), (size_t)item * 4},
+                {b->d_arena.p, b->arena.data(), b->arena.size()},
+                {b->d_tasks.p, b->tasks.data(), b->tasks.size() * sizeof(MxkTask)},
+                {b->d_plans.p, b->plans.data(), b->plans.size() * sizeof(CauchyPlanTask)}};
+    if (async_stream) {
+        size_t total = 0;
+        for (auto& u : ups) total += (u.bytes + 15) & ~(size_t)15;
+        if (total > b->upload.bytes) SCRS_CUDA(b->upload.ensure(total + total / 2));
+        uint8_t* h = b->upload.as<uint8_t>();
+        for (auto& u : ups) {
+            if (!u.bytes) continue;
+            memcpy(h, u.src, u.bytes);
+            SCRS_CUDA(cudaMemcpyAsync(u.dst, h, u.bytes, cudaMemcpyHostToDevice, stream));
+            h += (u.bytes + 15) & ~(size_t)15;
+        }
+    } else {
+        for (auto& u : ups)
+            if (u.bytes) SCRS_CUDA(cudaMemcpy(u.dst, u.src, u.bytes, cudaMemcpyHostToDevice));
+    }
     b->host_mode = false;  // scrs_stripe_batch_set_host re-enables it after this call
     if (b->graph) {  // geometry changed: the captured graph no longer applies
         cudaGraphExecDestroy(b->graph);

@@ -1083,6 +1083,18 @@ extern "C" void scrs_inc_reset(scrs_incremental_encoder* e) {
     e->fed_count = 0;
 }
 
+// Self-test of the device-side failure path (include/scrs_gpu.h).
+extern "C" int32_t scrs_selftest_wait_timeout(uint64_t limit_ns, scrs_error* err) {
+    if (limit_ns == 0 || limit_ns > 100000000ull) return set_err(err, SCRS_ERR_BAD_ARGUMENT, 1);
+    StatusWord sw;
+    SCRS_CUDA(sw.init());
+    OwnedStream st;
+    SCRS_CUDA(st.init());
+    SCRS_CUDA(launch_wait_selftest(sw.dev, limit_ns, st.s));
+    SCRS_CUDA(cudaStreamSynchronize(st.s));
+    return take_status(sw, err);
+}
+
 // Recipe-cache hits (repeated erasure patterns that skipped the plan launch).
 extern "C" uint64_t scrs_decode_scratch_recipe_hits(const scrs_decode_scratch* s) {
     return s ? s->recipe.hits : 0;

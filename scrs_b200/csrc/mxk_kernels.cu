@@ -454,6 +454,20 @@ __global__ void __launch_bounds__(kThreads, 8) mxk_single_kernel(const MxkTask T
     }
 }
 
+// ---- bounded-wait self-test -------------------------------------------------
+// Waits on an mbarrier that nothing arrives on: the bounded wait must give up
+// after limit_ns and report SCRS_ERR_DEVICE_TIMEOUT through the status word,
+// leaving the context usable.  No copy is in flight, so nothing is left to
+// drain before returning.
+__global__ void wait_selftest_kernel(int32_t* status, uint64_t limit_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+    mbar_wait_bounded(&bar, 0, status, limit_ns);
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&bar)) : "memory");
+}
+
 // ---- closed-form Cauchy solve on the device --------------------------------
 struct Gf8Tables {
     uint8_t log[256];
@@ -763,6 +777,11 @@ cudaError_t launch_gf16_mxk(const MxkTask* tasks, const uint32_t* item_task, uin
 cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream) {
     if (gf16) return launch_single_impl<1>(task, status, grid, stream);
     return launch_single_impl<0>(task, status, grid, stream);
+}
+
+cudaError_t launch_wait_selftest(int32_t* status, uint64_t limit_ns, cudaStream_t stream) {
+    wait_selftest_kernel<<<1, 32, 0, stream>>>(status, limit_ns);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_cauchy_plan_single(const CauchyPlanTask& task, int gf16, cudaStream_t stream) {

@@ -103,6 +103,8 @@ struct Slot {
 }  // namespace
 
 namespace scrs {
+int32_t stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc* descs, uint64_t count, bool async_stream,
+                              cudaStream_t stream, scrs_error* err);
 int32_t internal_batch_encoder_status(scrs_batch_encoder* e, scrs_error* err);
 int32_t internal_batch_decoder_status(scrs_batch_decoder* b, scrs_error* err);
 }  // namespace scrs
@@ -241,7 +243,9 @@ int32_t launch_group(Slot& sl, std::vector<Req>& group, scrs_error* err) {
         d[q].out = r.d.out;
         d[q].indices = r.d.op == SCRS_OP_DECODE ? r.idx16.data() : nullptr;
     }
-    int32_t rc = scrs_stripe_batch_set(sl.batch, d.data(), d.size(), err);
+    // uploads enqueued on the slot's stream: the slot is idle, so its previous
+    // run (which read the old batch contents) has finished
+    int32_t rc = stripe_batch_set_impl(sl.batch, d.data(), d.size(), true, sl.stream.s, err);
     if (rc) return rc;
     sl.used_batch = true;
     return scrs_stripe_batch_run(sl.batch, sl.stream.s, 0, err);

@@ -383,3 +383,30 @@ def test_recipe_cache_repeated_patterns(gpu, oracle, engine, k, m, L):
         lazy.finalize_into_with(out, ls)
         assert np.array_equal(out, data)
     assert ls.recipe_hits == 2
+
+
+def test_bounded_wait_reports_timeout_and_context_survives(gpu, oracle):
+    """A device wait that nothing completes gives up after its limit and reports
+    SCRS_ERR_DEVICE_TIMEOUT; the context keeps working afterwards."""
+    import ctypes as C
+    import time
+
+    from scrs_b200.api import _Error
+
+    lib = gpu.lib.lib
+    lib.scrs_selftest_wait_timeout.restype = C.c_int32
+    lib.scrs_selftest_wait_timeout.argtypes = [C.c_uint64, C.POINTER(_Error)]
+    for _ in range(2):
+        err = _Error()
+        t0 = time.monotonic()
+        rc = lib.scrs_selftest_wait_timeout(2_000_000, C.byref(err))
+        assert rc == 906 and err.code == 906
+        assert time.monotonic() - t0 < 5.0
+    err = _Error()
+    assert lib.scrs_selftest_wait_timeout(0, C.byref(err)) == 907
+    p = gpu.resolve(Engine.GOOD_CAUCHY, 10, 4, 4096)  # the context is still usable
+    data = gfpy.rng_bytes(10 * 4096, 5)
+    got, exp = np.zeros(4 * 4096, np.uint8), np.zeros(4 * 4096, np.uint8)
+    gpu.batch_encoder(p).encode_into(data, got)
+    oracle.batch_encoder(p).encode_into(data, exp)
+    assert np.array_equal(got, exp)
