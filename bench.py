@@ -535,9 +535,17 @@ def extra_afft(torch, api):
         torch.cuda.synchronize()
         assert torch.equal(out, data)
         t_dec = time_ms(torch, lambda: dec.decode_into_with((sel64, rows), out, ds), 3)
+        # few erasures (2 data symbols lost): the targeted path
+        few = np.array(list(range(2, k)) + [k, k + 1], dtype=np.uint64)
+        rows2 = word[torch.from_numpy(few.astype(np.int64)).cuda()].reshape(-1).contiguous()
+        dec.decode_into_with((few, rows2), out, ds)
+        torch.cuda.synchronize()
+        assert torch.equal(out, data)
+        t_few = time_ms(torch, lambda: dec.decode_into_with((few, rows2), out, ds), 5)
         res[tag] = {"k": k, "m": m, "symbol_len": La, "encode_GBps": round(k * La / t_enc / 1e6, 2),
                     "decode_GBps": round(k * La / t_dec / 1e6, 2), "encode_ms": round(t_enc, 3),
-                    "decode_ms": round(t_dec, 3)}
+                    "decode_ms": round(t_dec, 3), "decode_2_erasures_ms": round(t_few, 3),
+                    "decode_2_erasures_GBps": round(k * La / t_few / 1e6, 2)}
     return res
 
 

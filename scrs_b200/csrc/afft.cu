@@ -22,6 +22,7 @@ namespace {
 constexpr uint32_t kMult = 65535u;  // multiplicative group order (afft/decoder.rs:580)
 constexpr int kPassThreads = 256;
 constexpr int kTileBytes = 64 * 1024;
+constexpr uint32_t kTargetedMax = 5;  // TARGETED_MAX_MISSING (afft/decoder.rs:578)
 
 // ---- GF(2^16) log/exp tables in device memory (afft/decoder.rs:587-598) --------
 struct Log16Tables {
@@ -463,6 +464,91 @@ int32_t afft_locator_device(const uint8_t* d_known, uint32_t ts, uint32_t* wa, u
     return SCRS_OK;
 }
 
+// ---- targeted decode (afft/decoder.rs:360-441) --------------------------------
+// With r <= 5 missing data symbols and exactly r received repairs, the repairs
+// are linear in the data through the systematic generator rows
+// G[t][i] = L_S(e_t) / ((e_t + i) L_S'(i)) (generator_row, decoder.rs:600-619),
+// so the missing symbols are A^-1 (repairs + G_P d_P) with A = G restricted
+// to the missing columns: one k x r coefficient table and one multiply-XOR
+// pass instead of two transforms.
+__device__ __forceinline__ uint32_t lmul(const uint16_t* lg, const uint16_t* ex, uint32_t a, uint32_t b) {
+    if (!a || !b) return 0;
+    uint32_t e = (uint32_t)lg[a] + lg[b];
+    return ex[e >= kMult ? e - kMult : e];
+}
+__device__ __forceinline__ uint32_t linv(const uint16_t* lg, const uint16_t* ex, uint32_t a) {
+    return ex[(kMult - lg[a]) % kMult];
+}
+
+// gen[t*k + i] = G[t][i] for the r received repairs at evaluation points rep[t].
+__global__ void targeted_gen_kernel(const uint16_t* sys_values, const uint16_t* sys_derivs, const uint16_t* lg,
+                                    const uint16_t* ex, const uint16_t* rep, uint32_t r, uint32_t k, uint16_t* gen) {
+    for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < (uint64_t)r * k;
+         x += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t t = (uint32_t)(x / k), i = (uint32_t)(x - (uint64_t)t * k);
+        const uint32_t e = rep[t];
+        uint32_t lv = (uint32_t)lg[sys_values[e]] + 2 * kMult - lg[e ^ i] - lg[sys_derivs[i]];
+        gen[x] = ex[lv % kMult];
+    }
+}
+
+// One CTA: invert A (r x r, GF(2^16) Gauss-Jordan; invertible for every
+// supported pattern) and write the fused coefficients: rows 0..r-1 are the
+// received repairs (A^-1 columns), rows r.. the present data rows.
+__global__ void __launch_bounds__(256) targeted_solve_kernel(const uint16_t* gen, const uint16_t* missing,
+                                                             const uint16_t* present, uint32_t r, uint32_t k,
+                                                             const uint16_t* lg, const uint16_t* ex, uint16_t* coef,
+                                                             int32_t* status) {
+    __shared__ uint32_t inv[kTargetedMax][kTargetedMax];
+    if (threadIdx.x == 0) {
+        uint32_t a[kTargetedMax][2 * kTargetedMax];
+        for (uint32_t t = 0; t < r; t++)
+            for (uint32_t s = 0; s < r; s++) {
+                a[t][s] = gen[(size_t)t * k + missing[s]];
+                a[t][r + s] = t == s;
+            }
+        bool ok = true;
+        for (uint32_t col = 0; col < r && ok; col++) {
+            uint32_t piv = col;
+            while (piv < r && !a[piv][col]) piv++;
+            if (piv == r) {
+                ok = false;
+                break;
+            }
+            if (piv != col)
+                for (uint32_t q = 0; q < 2 * r; q++) {
+                    const uint32_t tmp = a[col][q];
+                    a[col][q] = a[piv][q];
+                    a[piv][q] = tmp;
+                }
+            const uint32_t pinv = linv(lg, ex, a[col][col]);
+            for (uint32_t q = 0; q < 2 * r; q++) a[col][q] = lmul(lg, ex, a[col][q], pinv);
+            for (uint32_t t = 0; t < r; t++) {
+                if (t == col || !a[t][col]) continue;
+                const uint32_t f = a[t][col];
+                for (uint32_t q = 0; q < 2 * r; q++) a[t][q] ^= lmul(lg, ex, f, a[col][q]);
+            }
+        }
+        if (!ok && status) atomicCAS(status, 0, SCRS_DECODE_INSUFFICIENT_RANK);
+        for (uint32_t s = 0; s < r; s++)
+            for (uint32_t t = 0; t < r; t++) inv[s][t] = ok ? a[s][r + t] : 0;  // inv[s][t] = (A^-1)[s][t]
+    }
+    __syncthreads();
+    // repair row t: output s gets (A^-1)[s][t]
+    for (uint32_t x = threadIdx.x; x < r * r; x += blockDim.x) {
+        const uint32_t t = x / r, s = x - t * r;
+        coef[(size_t)t * r + s] = (uint16_t)inv[s][t];
+    }
+    // present data row z (data index present[z]): output s gets sum_t (A^-1)[s][t] G[t][p]
+    for (uint32_t x = threadIdx.x; x < (k - r) * r; x += blockDim.x) {
+        const uint32_t z = x / r, s = x - z * r;
+        const uint32_t p = present[z];
+        uint32_t v = 0;
+        for (uint32_t t = 0; t < r; t++) v ^= lmul(lg, ex, inv[s][t], gen[(size_t)t * k + p]);
+        coef[(size_t)(r + z) * r + s] = (uint16_t)v;
+    }
+}
+
 // ---- AfftCodec -------------------------------------------------------------------
 int32_t AfftCodec::init(uint64_t k_, uint64_t m_, uint64_t L_, scrs_error* err) {
     k = k_, m = m_, L = L_, n = k + m;
@@ -493,7 +579,16 @@ int32_t AfftCodec::init(uint64_t k_, uint64_t m_, uint64_t L_, scrs_error* err) 
     int32_t r = afft_locator_device(known.as<uint8_t>(), (uint32_t)ts, wa.as<uint32_t>(), wb.as<uint32_t>(),
                                     enc_values.as<uint16_t>(), enc_derivs.as<uint16_t>(), 0, err);
     if (r) return r;
-    SCRS_CUDA(cudaStreamSynchronize(0));  // the locator ran on the legacy stream
+    // Systematic locator for the targeted decode: known = [k, ts), erased = [0, k).
+    SCRS_CUDA(sys_values.ensure(ts * 2));
+    SCRS_CUDA(sys_derivs.ensure(ts * 2));
+    SCRS_CUDA(cudaStreamSynchronize(0));  // `known` is rewritten below
+    for (uint64_t i = 0; i < ts; i++) hk[i] = i >= k ? 1 : 0;
+    SCRS_CUDA(cudaMemcpy(known.p, hk.data(), ts, cudaMemcpyHostToDevice));
+    r = afft_locator_device(known.as<uint8_t>(), (uint32_t)ts, wa.as<uint32_t>(), wb.as<uint32_t>(),
+                            sys_values.as<uint16_t>(), sys_derivs.as<uint16_t>(), 0, err);
+    if (r) return r;
+    SCRS_CUDA(cudaStreamSynchronize(0));  // the locators ran on the legacy stream
     return SCRS_OK;
 }
 
@@ -527,6 +622,9 @@ int32_t AfftWorkspace::init_decode(const AfftCodec& c, scrs_error* err) {
     host_known.assign(c.ts, 0);
     host_rows.assign(2 * c.k + 8, 0);
     SCRS_CUDA(rows.ensure(host_rows.size() * 2));
+    SCRS_CUDA(tgen.ensure(kTargetedMax * c.k * 2));
+    SCRS_CUDA(tcoef.ensure(kTargetedMax * c.k * 2));
+    SCRS_CUDA(tlists.ensure((3 * c.k + 4 * kTargetedMax + 8) * 2));
     return SCRS_OK;
 }
 
@@ -583,6 +681,8 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
         SCRS_CUDA(cudaGetLastError());
     }
     if (nm == 0) return SCRS_OK;
+    if (nm <= kTargetedMax) return decode_targeted(d_payloads, have, d_out, ws, status, st, err, row_map, miss, nm,
+                                                   pres, np);
     for (uint64_t i = 0; i < ts; i++) ws.host_known[i] = (i < n && have[i]) ? 1 : 0;
     SCRS_CUDA(cudaMemcpyAsync(ws.known.p, ws.host_known.data(), ts, cudaMemcpyHostToDevice, st));
     int32_t r = afft_locator_device(ws.known.as<uint8_t>(), (uint32_t)ts, ws.wht_a.as<uint32_t>(),
@@ -603,6 +703,63 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
     scale_out_kernel<<<grid_for((uint64_t)nm * G, 128), 128, 0, st>>>(ws.work1.as<uint8_t>(), G, L, d_miss, d_miss,
                                                                       nm, ws.derivs.as<uint16_t>(), lg, ex, d_out);
     SCRS_CUDA(cudaGetLastError());
+    return SCRS_OK;
+}
+
+int32_t AfftCodec::decode_targeted(const uint8_t* d_payloads, const uint8_t* have, uint8_t* d_out,
+                                   AfftWorkspace& ws, int32_t* status, cudaStream_t st, scrs_error* err,
+                                   const uint16_t* row_map, const uint16_t* miss, uint32_t nm, const uint16_t* pres,
+                                   uint32_t np) const {
+    const uint16_t *lg, *ex;
+    SCRS_CUDA(log16_tables(&lg, &ex));
+    // lists: in_rows[k] (repairs then present), out_rows[nm], rep[nm] (evaluation points),
+    // missing[nm], present[np]
+    std::vector<uint16_t> h(3 * k + 4 * kTargetedMax + 8, 0);
+    uint16_t* in_rows = h.data();
+    uint16_t* out_rows = in_rows + k;
+    uint16_t* rep = out_rows + kTargetedMax;
+    uint16_t* mis = rep + kTargetedMax;
+    uint16_t* prs = mis + kTargetedMax;
+    uint32_t nr = 0;
+    for (uint64_t w = k; w < n && nr < nm; w++)
+        if (have[w]) rep[nr++] = (uint16_t)w;
+    if (nr != nm) return set_err(err, SCRS_DECODE_INSUFFICIENT_RANK, k, k - nm + nr);
+    auto payload_row = [&](uint32_t w) { return row_map ? row_map[w] : (uint16_t)w; };
+    for (uint32_t t = 0; t < nm; t++) in_rows[t] = payload_row(rep[t]), out_rows[t] = miss[t], mis[t] = miss[t];
+    for (uint32_t z = 0; z < np; z++) in_rows[nm + z] = payload_row(pres[z]), prs[z] = pres[z];
+    SCRS_CUDA(cudaMemcpyAsync(ws.tlists.p, h.data(), h.size() * 2, cudaMemcpyHostToDevice, st));
+    const uint16_t* d_in_rows = ws.tlists.as<uint16_t>();
+    const uint16_t* d_out_rows = d_in_rows + k;
+    const uint16_t* d_rep = d_out_rows + kTargetedMax;
+    const uint16_t* d_mis = d_rep + kTargetedMax;
+    const uint16_t* d_prs = d_mis + kTargetedMax;
+    targeted_gen_kernel<<<grid_for((uint64_t)nm * k, 256), 256, 0, st>>>(
+        sys_values.as<uint16_t>(), sys_derivs.as<uint16_t>(), lg, ex, d_rep, nm, (uint32_t)k, ws.tgen.as<uint16_t>());
+    SCRS_CUDA(cudaGetLastError());
+    targeted_solve_kernel<<<1, 256, 0, st>>>(ws.tgen.as<uint16_t>(), d_mis, d_prs, nm, (uint32_t)k, lg, ex,
+                                             ws.tcoef.as<uint16_t>(), status);
+    SCRS_CUDA(cudaGetLastError());
+    MxkTask T{};
+    T.in = d_payloads;
+    T.out = d_out;
+    T.coef = ws.tcoef.p;
+    T.in_rows = d_in_rows;
+    T.out_rows = d_out_rows;
+    T.L = L;
+    T.in_stride = L;
+    T.out_stride = L;
+    T.n_in = (uint32_t)k;
+    T.n_out = nm;
+    T.ld = nm;
+    T.n_items = n_chunks(L, true);
+    T.aligned = (L % 16 == 0 && aligned16(d_payloads) && aligned16(d_out)) ? 1u : 0u;
+    const bool atomics_ok = L % 4 == 0 && (reinterpret_cast<uintptr_t>(d_out) & 3u) == 0;
+    if (atomics_ok) {
+        for (uint32_t t = 0; t < nm; t++) SCRS_CUDA(cudaMemsetAsync(d_out + (uint64_t)miss[t] * L, 0, L, st));
+        SCRS_CUDA(launch_mxk_ksplit(T, 1, status, st));
+    } else {
+        SCRS_CUDA(launch_mxk_single(T, 1, status, 0, st));
+    }
     return SCRS_OK;
 }
 

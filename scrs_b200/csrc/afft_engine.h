@@ -33,11 +33,19 @@ class AfftCodec {
     int32_t decode(const uint8_t* d_payloads, const uint8_t* have, uint8_t* d_out, AfftWorkspace& ws,
                    int32_t* status, cudaStream_t st, scrs_error* err, const uint16_t* row_map = nullptr) const;
 
+    // r <= 5 missing data symbols: one coefficient table + multiply-XOR pass.
+    int32_t decode_targeted(const uint8_t* d_payloads, const uint8_t* have, uint8_t* d_out, AfftWorkspace& ws,
+                            int32_t* status, cudaStream_t st, scrs_error* err, const uint16_t* row_map,
+                            const uint16_t* miss, uint32_t nm, const uint16_t* pres, uint32_t np) const;
+
     uint64_t k = 0, m = 0, n = 0, L = 0, padded_k = 0, ts = 0;
     uint32_t log_ts = 0;
     DevBuf factors;                 // uint16[ts], heap layout (transform.rs:30-61)
     uint16_t deriv_factors[16] = {};
     DevBuf enc_values, enc_derivs;  // encode locator for E = [k, ts): uint16[ts]
+    // Systematic locator L_S(x) = prod_{i<k}(x + i) (decoder.rs:256-266):
+    // sys_values[e] = L_S(e) for e >= k, sys_derivs[i] = L_S'(i) for i < k.
+    DevBuf sys_values, sys_derivs;
 };
 
 class AfftWorkspace {
@@ -50,6 +58,7 @@ class AfftWorkspace {
     DevBuf values, derivs;          // uint16[ts]
     DevBuf rows;                    // uint16 lists for the output stage
     DevBuf row_map;                 // uint16[n] codeword index -> payload row
+    DevBuf tgen, tcoef, tlists;     // targeted decode: generator rows, fused coefficients, lists
     std::vector<uint8_t> host_known;
     std::vector<uint16_t> host_rows;
     uint64_t k = 0, m = 0, L = 0;

@@ -76,6 +76,10 @@ cudaError_t launch_gf16_mxk(const MxkTask* tasks, const uint32_t* item_task, uin
 // One task by value; grid <= 0 means one CTA per row chunk.
 cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream);
 cudaError_t launch_cauchy_plan_single(const CauchyPlanTask& task, int gf16, cudaStream_t stream);
+// Many inputs, few outputs: inputs split into blocks over CTAs, partial sums
+// XORed (atomicXor) into outputs that must be zero beforehand; T.n_out <= 64,
+// no accumulate mode.  Pass-through copies as in launch_mxk_single.
+cudaError_t launch_mxk_ksplit(const MxkTask& task, int gf16, int32_t* status, cudaStream_t stream);
 // One bounded wait that nothing completes (limit_ns of global time).
 cudaError_t launch_wait_selftest(int32_t* status, uint64_t limit_ns, cudaStream_t stream);
 // max_r: the largest r among the tasks (all of them, with or without `work`).

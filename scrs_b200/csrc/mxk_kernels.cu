@@ -206,7 +206,7 @@ __device__ __forceinline__ void load_out_planes(const uint8_t* orow, uint64_t of
 template <int kGf16>
 __device__ __forceinline__ void output_row(const uint8_t* buf, uint32_t c, uint16_t* steps, uint32_t seg_n, int lane,
                                            bool existing, uint8_t* orow, uint64_t off, uint64_t L, bool aligned,
-                                           bool full) {
+                                           bool full, bool atomic_out) {
     using G = FieldGeom<kGf16>;
     using Words = typename Lane<kGf16>::Words;
     constexpr int kWords = Lane<kGf16>::kWords;
@@ -267,6 +267,16 @@ __device__ __forceinline__ void output_row(const uint8_t* buf, uint32_t c, uint1
     }
     __syncwarp();  // the list is rebuilt for the warp's next output row
     bitslice_lane<kGf16>(acc);
+    if (atomic_out) {  // partial sum of an input range: XOR into the (zeroed) output
+#pragma unroll
+        for (int pc = 0; pc < Lane<kGf16>::kPieces; pc++) {
+            const uint64_t pos = off + piece_pos(pc, lane);
+#pragma unroll
+            for (int w = 0; w < 4; w++)
+                if (pos + 4 * w + 4 <= L) atomicXor(reinterpret_cast<unsigned int*>(orow + pos + 4 * w), acc[4 * pc + w]);
+        }
+        return;
+    }
     store_pieces<Lane<kGf16>::kPieces>(orow, off, 0, lane, L, aligned, full, acc);
 }
 
@@ -276,7 +286,8 @@ __device__ __forceinline__ void output_row(const uint8_t* buf, uint32_t c, uint1
 template <int kGf16>
 __device__ bool process_item(const MxkTask& T, uint32_t chunk, uint8_t* buf, uint8_t* steps_base, uint64_t* bar,
                              uint32_t& phase, int seg_cap, int32_t* status, uint32_t out_lo, uint32_t out_hi,
-                             bool first_issued) {
+                             bool first_issued, uint32_t in_lo = 0, uint32_t in_hi = 0xFFFFFFFFu,
+                             bool atomic_out = false) {
     using G = FieldGeom<kGf16>;
     constexpr int kPieces = Lane<kGf16>::kPieces;
     // GF(256) rows are bit-sliced in two independent 32-byte halves per lane,
@@ -286,7 +297,7 @@ __device__ bool process_item(const MxkTask& T, uint32_t chunk, uint8_t* buf, uin
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint64_t L = T.L;
     const uint64_t off = (uint64_t)chunk * G::kChunk;
-    const uint32_t n_in = T.n_in;
+    const uint32_t n_in = umin32(T.n_in, in_hi);
     const bool aligned = T.aligned != 0;
     const bool full = aligned && off + G::kChunk <= L;
     uint16_t* steps = reinterpret_cast<uint16_t*>(steps_base + warp * kStepBytes);
@@ -295,9 +306,9 @@ __device__ bool process_item(const MxkTask& T, uint32_t chunk, uint8_t* buf, uin
         const uint32_t og_n = out_hi > og ? umin32(kMaxOutGroup, out_hi - og) : 0;
         const bool need_pass = og == 0 && T.pass_rows != nullptr;
         if (og_n == 0 && !need_pass) break;
-        for (uint32_t seg = 0; seg < n_in; seg += seg_cap) {
+        for (uint32_t seg = in_lo; seg < n_in; seg += seg_cap) {
             const uint32_t seg_n = umin32((uint32_t)seg_cap, n_in - seg);
-            const bool prefetched = first_issued && og == out_lo && seg == 0;
+            const bool prefetched = first_issued && og == out_lo && seg == in_lo;
             // this warp's first output's coefficients, loaded while the rows arrive
             uint32_t c = (uint32_t)warp < og_n ? lane_coef<kGf16>(T, seg, seg_n, og, warp, lane) : 0u;
             // ---- stage the segment's rows in shared memory
@@ -351,8 +362,8 @@ __device__ bool process_item(const MxkTask& T, uint32_t chunk, uint8_t* buf, uin
             for (uint32_t j = warp; j < og_n; j += 4) {
                 if (j != (uint32_t)warp) c = lane_coef<kGf16>(T, seg, seg_n, og, j, lane);
                 const uint32_t orow_idx = T.out_rows ? T.out_rows[og + j] : og + j;
-                output_row<kGf16>(buf, c, steps, seg_n, lane, seg != 0 || T.accumulate,
-                                  T.out + (uint64_t)orow_idx * T.out_stride, off, L, aligned, full);
+                output_row<kGf16>(buf, c, steps, seg_n, lane, !atomic_out && (seg != in_lo || T.accumulate),
+                                  T.out + (uint64_t)orow_idx * T.out_stride, off, L, aligned, full, atomic_out);
             }
             __syncthreads();
         }
@@ -450,6 +461,32 @@ __global__ void __launch_bounds__(kThreads, 8) mxk_single_kernel(const MxkTask T
         const uint32_t chunk = item % T.n_items, sp = item / T.n_items;
         const uint32_t lo = sp * per, hi = min(T.n_out, lo + per);
         if (!process_item<kGf16>(T, chunk, S.buf, S.steps, S.bar, phase, seg_cap, status, lo, hi, false)) break;
+        __syncthreads();
+    }
+}
+
+// Few outputs, many inputs (the AFFT targeted decode: r <= 5 outputs from k
+// inputs): items are (row chunk, block of seg_cap inputs); each CTA XORs its
+// block's partial sums into the zero-initialised outputs with atomicXor, so
+// all blocks run in parallel instead of one CTA walking every segment.
+template <int kGf16>
+__global__ void __launch_bounds__(kThreads, 8) mxk_ksplit_kernel(const MxkTask T, int32_t* status, int seg_cap) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    const SmemLayout S = layout<kGf16>(smem, seg_cap);
+    if (threadIdx.x == 0) {
+        mbar_init(S.bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    const uint32_t blocks = (T.n_in + seg_cap - 1) / seg_cap;
+    const uint32_t items = T.n_items * blocks;
+    for (uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
+        const uint32_t chunk = item % T.n_items, blk = item / T.n_items;
+        const uint32_t lo = blk * (uint32_t)seg_cap;
+        if (!process_item<kGf16>(T, chunk, S.buf, S.steps, S.bar, phase, seg_cap, status, 0, T.n_out, false, lo,
+                                 lo + (uint32_t)seg_cap, true))
+            break;
         __syncthreads();
     }
 }
@@ -777,6 +814,26 @@ cudaError_t launch_gf16_mxk(const MxkTask* tasks, const uint32_t* item_task, uin
 cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream) {
     if (gf16) return launch_single_impl<1>(task, status, grid, stream);
     return launch_single_impl<0>(task, status, grid, stream);
+}
+
+cudaError_t launch_mxk_ksplit(const MxkTask& T, int gf16, int32_t* status, cudaStream_t stream) {
+    if (T.n_items == 0 || T.n_in == 0) return cudaSuccess;
+    const int seg_cap = std::max(1, std::min((int)T.n_in, gf16 ? FieldGeom<1>::kSeg : FieldGeom<0>::kSeg));
+    const uint32_t items = T.n_items * ((T.n_in + seg_cap - 1) / seg_cap);
+    const int grid = (int)std::min<uint32_t>(items, 148u * 8u);
+    const size_t smem = smem_bytes(gf16, seg_cap);
+    if (gf16) {
+        cudaError_t e = cudaFuncSetAttribute(mxk_ksplit_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem_bytes(1, FieldGeom<1>::kSeg));
+        if (e != cudaSuccess) return e;
+        mxk_ksplit_kernel<1><<<grid, kThreads, smem, stream>>>(T, status, seg_cap);
+    } else {
+        cudaError_t e = cudaFuncSetAttribute(mxk_ksplit_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem_bytes(0, FieldGeom<0>::kSeg));
+        if (e != cudaSuccess) return e;
+        mxk_ksplit_kernel<0><<<grid, kThreads, smem, stream>>>(T, status, seg_cap);
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_wait_selftest(int32_t* status, uint64_t limit_ns, cudaStream_t stream) {

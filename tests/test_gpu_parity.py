@@ -216,6 +216,27 @@ def test_afft_random_and_large_patterns(gpu, oracle):
     assert np.array_equal(lazy_decode(gpu, p, word, sel), data)
 
 
+@pytest.mark.parametrize("k,m,L", [(4096, 64, 1024), (1000, 24, 258), (37, 11, 6), (2048, 8, 4096)])
+def test_afft_targeted_few_erasures(gpu, oracle, k, m, L):
+    """r <= 5 missing data symbols take the targeted path (one coefficient
+    table + multiply-XOR over all k inputs); r = 6 the full transforms.  Both
+    must recover the data exactly, through the lazy and the batch decoders,
+    for aligned and odd symbol lengths."""
+    p = gpu.resolve(Engine.AFFT, k, m, L)
+    data = gfpy.rng_bytes(k * L, k + L)
+    word = encode_word(oracle, p, data)
+    rng = np.random.default_rng(k)
+    for r in (1, 2, 3, 4, 5, 6):
+        if r > m:
+            continue
+        erased = set(rng.choice(k, r, replace=False).tolist())
+        reps = (k + rng.choice(m, r, replace=False)).tolist()
+        sub = [i for i in range(k) if i not in erased] + reps
+        order = rng.permutation(sub).tolist()
+        assert np.array_equal(batch_decode(gpu, p, word, order), data), r
+        assert np.array_equal(lazy_decode(gpu, p, word, order), data), r
+
+
 # ---------------------------------------------------------------- device-pointer forms
 
 def test_device_pointer_entry_points(gpu, oracle):
