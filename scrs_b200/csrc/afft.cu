@@ -492,60 +492,63 @@ __global__ void targeted_gen_kernel(const uint16_t* sys_values, const uint16_t* 
     }
 }
 
-// One CTA: invert A (r x r, GF(2^16) Gauss-Jordan; invertible for every
-// supported pattern) and write the fused coefficients: rows 0..r-1 are the
-// received repairs (A^-1 columns), rows r.. the present data rows.
-__global__ void __launch_bounds__(256) targeted_solve_kernel(const uint16_t* gen, const uint16_t* missing,
-                                                             const uint16_t* present, uint32_t r, uint32_t k,
-                                                             const uint16_t* lg, const uint16_t* ex, uint16_t* coef,
-                                                             int32_t* status) {
-    __shared__ uint32_t inv[kTargetedMax][kTargetedMax];
-    if (threadIdx.x == 0) {
-        uint32_t a[kTargetedMax][2 * kTargetedMax];
-        for (uint32_t t = 0; t < r; t++)
-            for (uint32_t s = 0; s < r; s++) {
-                a[t][s] = gen[(size_t)t * k + missing[s]];
-                a[t][r + s] = t == s;
-            }
-        bool ok = true;
-        for (uint32_t col = 0; col < r && ok; col++) {
-            uint32_t piv = col;
-            while (piv < r && !a[piv][col]) piv++;
-            if (piv == r) {
-                ok = false;
-                break;
-            }
-            if (piv != col)
-                for (uint32_t q = 0; q < 2 * r; q++) {
-                    const uint32_t tmp = a[col][q];
-                    a[col][q] = a[piv][q];
-                    a[piv][q] = tmp;
-                }
-            const uint32_t pinv = linv(lg, ex, a[col][col]);
-            for (uint32_t q = 0; q < 2 * r; q++) a[col][q] = lmul(lg, ex, a[col][q], pinv);
-            for (uint32_t t = 0; t < r; t++) {
-                if (t == col || !a[t][col]) continue;
-                const uint32_t f = a[t][col];
-                for (uint32_t q = 0; q < 2 * r; q++) a[t][q] ^= lmul(lg, ex, f, a[col][q]);
-            }
+// One thread: invert A (r x r, GF(2^16) Gauss-Jordan; invertible for every
+// supported pattern) into inv[s*r + t] = (A^-1)[s][t].
+__global__ void targeted_invert_kernel(const uint16_t* gen, const uint16_t* missing, uint32_t r, uint32_t k,
+                                       const uint16_t* lg, const uint16_t* ex, uint16_t* inv, int32_t* status) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint32_t a[kTargetedMax][2 * kTargetedMax];
+    for (uint32_t t = 0; t < r; t++)
+        for (uint32_t s = 0; s < r; s++) {
+            a[t][s] = gen[(size_t)t * k + missing[s]];
+            a[t][r + s] = t == s;
         }
-        if (!ok && status) atomicCAS(status, 0, SCRS_DECODE_INSUFFICIENT_RANK);
-        for (uint32_t s = 0; s < r; s++)
-            for (uint32_t t = 0; t < r; t++) inv[s][t] = ok ? a[s][r + t] : 0;  // inv[s][t] = (A^-1)[s][t]
+    bool ok = true;
+    for (uint32_t col = 0; col < r && ok; col++) {
+        uint32_t piv = col;
+        while (piv < r && !a[piv][col]) piv++;
+        if (piv == r) {
+            ok = false;
+            break;
+        }
+        if (piv != col)
+            for (uint32_t q = 0; q < 2 * r; q++) {
+                const uint32_t tmp = a[col][q];
+                a[col][q] = a[piv][q];
+                a[piv][q] = tmp;
+            }
+        const uint32_t pinv = linv(lg, ex, a[col][col]);
+        for (uint32_t q = 0; q < 2 * r; q++) a[col][q] = lmul(lg, ex, a[col][q], pinv);
+        for (uint32_t t = 0; t < r; t++) {
+            if (t == col || !a[t][col]) continue;
+            const uint32_t f = a[t][col];
+            for (uint32_t q = 0; q < 2 * r; q++) a[t][q] ^= lmul(lg, ex, f, a[col][q]);
+        }
     }
+    if (!ok && status) atomicCAS(status, 0, SCRS_DECODE_INSUFFICIENT_RANK);
+    for (uint32_t s = 0; s < r; s++)
+        for (uint32_t t = 0; t < r; t++) inv[s * r + t] = ok ? (uint16_t)a[s][r + t] : 0;
+}
+
+// Fused coefficients, rows 0..r-1 the received repairs (A^-1 columns), rows
+// r.. the present data rows: row z, output s = sum_t (A^-1)[s][t] G[t][present[z]].
+__global__ void targeted_fuse_kernel(const uint16_t* gen, const uint16_t* inv_g, const uint16_t* present, uint32_t r,
+                                     uint32_t k, const uint16_t* lg, const uint16_t* ex, uint16_t* coef) {
+    __shared__ uint32_t inv[kTargetedMax * kTargetedMax];
+    for (uint32_t x = threadIdx.x; x < r * r; x += blockDim.x) inv[x] = inv_g[x];
     __syncthreads();
-    // repair row t: output s gets (A^-1)[s][t]
-    for (uint32_t x = threadIdx.x; x < r * r; x += blockDim.x) {
-        const uint32_t t = x / r, s = x - t * r;
-        coef[(size_t)t * r + s] = (uint16_t)inv[s][t];
-    }
-    // present data row z (data index present[z]): output s gets sum_t (A^-1)[s][t] G[t][p]
-    for (uint32_t x = threadIdx.x; x < (k - r) * r; x += blockDim.x) {
-        const uint32_t z = x / r, s = x - z * r;
-        const uint32_t p = present[z];
-        uint32_t v = 0;
-        for (uint32_t t = 0; t < r; t++) v ^= lmul(lg, ex, inv[s][t], gen[(size_t)t * k + p]);
-        coef[(size_t)(r + z) * r + s] = (uint16_t)v;
+    for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < (uint64_t)k * r;
+         x += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t row = (uint32_t)(x / r), s = (uint32_t)(x - (uint64_t)row * r);
+        uint32_t v;
+        if (row < r) {
+            v = inv[s * r + row];
+        } else {
+            const uint32_t p = present[row - r];
+            v = 0;
+            for (uint32_t t = 0; t < r; t++) v ^= lmul(lg, ex, inv[s * r + t], gen[(size_t)t * k + p]);
+        }
+        coef[x] = (uint16_t)v;
     }
 }
 
@@ -624,7 +627,7 @@ int32_t AfftWorkspace::init_decode(const AfftCodec& c, scrs_error* err) {
     SCRS_CUDA(rows.ensure(host_rows.size() * 2));
     SCRS_CUDA(tgen.ensure(kTargetedMax * c.k * 2));
     SCRS_CUDA(tcoef.ensure(kTargetedMax * c.k * 2));
-    SCRS_CUDA(tlists.ensure((3 * c.k + 4 * kTargetedMax + 8) * 2));
+    SCRS_CUDA(tlists.ensure((3 * c.k + 4 * kTargetedMax + kTargetedMax * kTargetedMax + 8) * 2));
     return SCRS_OK;
 }
 
@@ -714,7 +717,7 @@ int32_t AfftCodec::decode_targeted(const uint8_t* d_payloads, const uint8_t* hav
     SCRS_CUDA(log16_tables(&lg, &ex));
     // lists: in_rows[k] (repairs then present), out_rows[nm], rep[nm] (evaluation points),
     // missing[nm], present[np]
-    std::vector<uint16_t> h(3 * k + 4 * kTargetedMax + 8, 0);
+    std::vector<uint16_t> h(3 * k + 4 * kTargetedMax + kTargetedMax * kTargetedMax + 8, 0);
     uint16_t* in_rows = h.data();
     uint16_t* out_rows = in_rows + k;
     uint16_t* rep = out_rows + kTargetedMax;
@@ -736,8 +739,11 @@ int32_t AfftCodec::decode_targeted(const uint8_t* d_payloads, const uint8_t* hav
     targeted_gen_kernel<<<grid_for((uint64_t)nm * k, 256), 256, 0, st>>>(
         sys_values.as<uint16_t>(), sys_derivs.as<uint16_t>(), lg, ex, d_rep, nm, (uint32_t)k, ws.tgen.as<uint16_t>());
     SCRS_CUDA(cudaGetLastError());
-    targeted_solve_kernel<<<1, 256, 0, st>>>(ws.tgen.as<uint16_t>(), d_mis, d_prs, nm, (uint32_t)k, lg, ex,
-                                             ws.tcoef.as<uint16_t>(), status);
+    uint16_t* d_inv = const_cast<uint16_t*>(d_prs) + k;  // r*r entries after the present list
+    targeted_invert_kernel<<<1, 32, 0, st>>>(ws.tgen.as<uint16_t>(), d_mis, nm, (uint32_t)k, lg, ex, d_inv, status);
+    SCRS_CUDA(cudaGetLastError());
+    targeted_fuse_kernel<<<grid_for((uint64_t)k * nm, 256), 256, 0, st>>>(ws.tgen.as<uint16_t>(), d_inv, d_prs, nm,
+                                                                         (uint32_t)k, lg, ex, ws.tcoef.as<uint16_t>());
     SCRS_CUDA(cudaGetLastError());
     MxkTask T{};
     T.in = d_payloads;
@@ -753,13 +759,9 @@ int32_t AfftCodec::decode_targeted(const uint8_t* d_payloads, const uint8_t* hav
     T.ld = nm;
     T.n_items = n_chunks(L, true);
     T.aligned = (L % 16 == 0 && aligned16(d_payloads) && aligned16(d_out)) ? 1u : 0u;
-    const bool atomics_ok = L % 4 == 0 && (reinterpret_cast<uintptr_t>(d_out) & 3u) == 0;
-    if (atomics_ok) {
-        for (uint32_t t = 0; t < nm; t++) SCRS_CUDA(cudaMemsetAsync(d_out + (uint64_t)miss[t] * L, 0, L, st));
-        SCRS_CUDA(launch_mxk_ksplit(T, 1, status, st));
-    } else {
-        SCRS_CUDA(launch_mxk_single(T, 1, status, 0, st));
-    }
+    // k inputs: the launch splits them over CTAs (input-split form) when the
+    // output rows allow 4-byte atomics, else walks them per chunk
+    SCRS_CUDA(launch_mxk_single(T, 1, status, 0, st));
     return SCRS_OK;
 }
 

@@ -94,18 +94,27 @@ struct RecipeBufs {
                 *fresh = false;
                 return cudaSuccess;
             }
+        const size_t need = (size_t)k * std::max<size_t>(missing.size(), 1) * elem;
         Entry* slot = nullptr;
         if (cache.size() < kCacheEntries) {
             cache.emplace_back(new Entry());
             slot = cache.back().get();
         } else {
-            slot = cache[0].get();
+            // the least recently used entry whose buffer is large enough, so a
+            // reuse does not reallocate (cudaFree would wait for the device)
             for (auto& e : cache)
-                if (e->last_use < slot->last_use) slot = e.get();
+                if (e->coef.bytes >= need && (!slot || e->last_use < slot->last_use)) slot = e.get();
+            if (!slot) {
+                slot = cache[0].get();
+                for (auto& e : cache)
+                    if (e->last_use < slot->last_use) slot = e.get();
+            }
         }
         // Reusing a buffer that a queued kernel may still read is safe: its
         // pattern's plan and multiply ran earlier on the same stream.
-        cudaError_t e = slot->coef.ensure((size_t)k * std::max<size_t>(missing.size(), 1) * elem);
+        // new buffers get room for up to 16 erasures, so later patterns fit
+        const size_t room = (size_t)k * std::min<size_t>(std::max<size_t>(rmax, 1), 16) * elem;
+        cudaError_t e = slot->coef.ensure(slot->coef.p ? need : std::max(need, room));
         if (e != cudaSuccess) {
             slot->key.clear();
             return e;

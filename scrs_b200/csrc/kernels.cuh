@@ -73,12 +73,14 @@ cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, ui
                              uint32_t* work_counter, int32_t* status, int max_in, int grid, cudaStream_t stream);
 cudaError_t launch_gf16_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
                             uint32_t* work_counter, int32_t* status, int max_in, int grid, cudaStream_t stream);
-// One task by value; grid <= 0 means one CTA per row chunk.
+// One task by value; grid <= 0 means one CTA per row chunk (or the
+// input-split form for more than one segment of inputs, see below).
 cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream);
 cudaError_t launch_cauchy_plan_single(const CauchyPlanTask& task, int gf16, cudaStream_t stream);
-// Many inputs, few outputs: inputs split into blocks over CTAs, partial sums
-// XORed (atomicXor) into outputs that must be zero beforehand; T.n_out <= 64,
-// no accumulate mode.  Pass-through copies as in launch_mxk_single.
+// Input-split form: inputs split into blocks over CTAs, partial sums XORed
+// (atomicXor) into the outputs, which the launch zeroes first unless the task
+// accumulates; needs L and the output rows 4-byte aligned.  launch_mxk_single
+// takes this form by itself when a task has more than one segment of inputs.
 cudaError_t launch_mxk_ksplit(const MxkTask& task, int gf16, int32_t* status, cudaStream_t stream);
 // One bounded wait that nothing completes (limit_ns of global time).
 cudaError_t launch_wait_selftest(int32_t* status, uint64_t limit_ns, cudaStream_t stream);

@@ -465,12 +465,14 @@ __global__ void __launch_bounds__(kThreads, 8) mxk_single_kernel(const MxkTask T
     }
 }
 
-// Few outputs, many inputs (the AFFT targeted decode: r <= 5 outputs from k
-// inputs): items are (row chunk, block of seg_cap inputs); each CTA XORs its
-// block's partial sums into the zero-initialised outputs with atomicXor, so
-// all blocks run in parallel instead of one CTA walking every segment.
+// Many inputs: items are (row chunk, output range of `per` outputs, block of
+// seg_cap inputs); each CTA XORs its block's partial sums into the outputs
+// with atomicXor (outputs zeroed beforehand unless accumulating), so all
+// input blocks run in parallel instead of one CTA walking every segment and
+// re-reading its partial sums.
 template <int kGf16>
-__global__ void __launch_bounds__(kThreads, 8) mxk_ksplit_kernel(const MxkTask T, int32_t* status, int seg_cap) {
+__global__ void __launch_bounds__(kThreads, 8) mxk_ksplit_kernel(const MxkTask T, int32_t* status, int seg_cap,
+                                                                 uint32_t per) {
     extern __shared__ __align__(128) uint8_t smem[];
     const SmemLayout S = layout<kGf16>(smem, seg_cap);
     if (threadIdx.x == 0) {
@@ -480,14 +482,28 @@ __global__ void __launch_bounds__(kThreads, 8) mxk_ksplit_kernel(const MxkTask T
     __syncthreads();
     uint32_t phase = 0;
     const uint32_t blocks = (T.n_in + seg_cap - 1) / seg_cap;
-    const uint32_t items = T.n_items * blocks;
+    const uint32_t splits = T.n_out ? (T.n_out + per - 1) / per : 1;
+    const uint32_t items = T.n_items * splits * blocks;
     for (uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
-        const uint32_t chunk = item % T.n_items, blk = item / T.n_items;
+        const uint32_t chunk = item % T.n_items, rest = item / T.n_items;
+        const uint32_t sp = rest % splits, blk = rest / splits;
         const uint32_t lo = blk * (uint32_t)seg_cap;
-        if (!process_item<kGf16>(T, chunk, S.buf, S.steps, S.bar, phase, seg_cap, status, 0, T.n_out, false, lo,
+        const uint32_t olo = sp * per, ohi = min(T.n_out, olo + per);
+        if (!process_item<kGf16>(T, chunk, S.buf, S.steps, S.bar, phase, seg_cap, status, olo, ohi, false, lo,
                                  lo + (uint32_t)seg_cap, true))
             break;
         __syncthreads();
+    }
+}
+
+// Zero the output rows of T (4-byte words; L % 4 == 0).
+__global__ void zero_out_rows_kernel(const MxkTask T) {
+    const uint64_t words = T.L / 4;
+    for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < (uint64_t)T.n_out * words;
+         x += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t j = (uint32_t)(x / words);
+        const uint32_t r = T.out_rows ? T.out_rows[j] : j;
+        reinterpret_cast<uint32_t*>(T.out + (uint64_t)r * T.out_stride)[x - (uint64_t)j * words] = 0;
     }
 }
 
@@ -751,6 +767,38 @@ cudaError_t set_mxk_attrs() {
     return e;
 }
 
+// Input-split launch (see mxk_ksplit_kernel): outputs are zeroed first unless
+// the task accumulates; about four outputs per item.
+template <int kGf16>
+cudaError_t launch_ksplit_impl(const MxkTask& T, int32_t* status, cudaStream_t stream) {
+    using G = FieldGeom<kGf16>;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(mxk_ksplit_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem_bytes(kGf16, G::kSeg));
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    if (!T.accumulate && T.n_out) {
+        const uint64_t words = (uint64_t)T.n_out * (T.L / 4);
+        zero_out_rows_kernel<<<(int)std::min<uint64_t>((words + 255) / 256, 148 * 16), 256, 0, stream>>>(T);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    const int seg_cap = std::max(1, std::min((int)T.n_in, G::kSeg));
+    const uint32_t per = std::max<uint32_t>(1, std::min<uint32_t>(T.n_out, 4));
+    const uint32_t splits = T.n_out ? (T.n_out + per - 1) / per : 1;
+    const uint64_t items = (uint64_t)T.n_items * splits * ((T.n_in + seg_cap - 1) / seg_cap);
+    const int grid = (int)std::min<uint64_t>(items, 148u * 8u);
+    mxk_ksplit_kernel<kGf16><<<grid, kThreads, smem_bytes(kGf16, seg_cap), stream>>>(T, status, seg_cap, per);
+    return cudaGetLastError();
+}
+
+// Whether partial sums of T's outputs can be combined with 4-byte atomicXor.
+bool ksplit_ok(const MxkTask& T) {
+    return T.L % 4 == 0 && T.out_stride % 4 == 0 && (reinterpret_cast<uintptr_t>(T.out) & 3u) == 0 && T.n_out > 0;
+}
+
 template <int kGf16>
 cudaError_t launch_single_impl(const MxkTask& T, int32_t* status, int grid, cudaStream_t stream) {
     using G = FieldGeom<kGf16>;
@@ -758,6 +806,8 @@ cudaError_t launch_single_impl(const MxkTask& T, int32_t* status, int grid, cuda
     cudaError_t e = set_mxk_attrs<kGf16>();
     if (e != cudaSuccess) return e;
     int seg_cap = std::max(1, std::min((int)T.n_in, G::kSeg));
+    // More than one segment of inputs: split the inputs over CTAs instead.
+    if ((int)T.n_in > seg_cap && ksplit_ok(T)) return launch_ksplit_impl<kGf16>(T, status, stream);
     // Split the outputs when the row chunks alone cannot fill the GPU, keeping
     // at least one output per warp in each split (every split re-stages and
     // re-slices the chunk's input rows).
@@ -818,22 +868,8 @@ cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, in
 
 cudaError_t launch_mxk_ksplit(const MxkTask& T, int gf16, int32_t* status, cudaStream_t stream) {
     if (T.n_items == 0 || T.n_in == 0) return cudaSuccess;
-    const int seg_cap = std::max(1, std::min((int)T.n_in, gf16 ? FieldGeom<1>::kSeg : FieldGeom<0>::kSeg));
-    const uint32_t items = T.n_items * ((T.n_in + seg_cap - 1) / seg_cap);
-    const int grid = (int)std::min<uint32_t>(items, 148u * 8u);
-    const size_t smem = smem_bytes(gf16, seg_cap);
-    if (gf16) {
-        cudaError_t e = cudaFuncSetAttribute(mxk_ksplit_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem_bytes(1, FieldGeom<1>::kSeg));
-        if (e != cudaSuccess) return e;
-        mxk_ksplit_kernel<1><<<grid, kThreads, smem, stream>>>(T, status, seg_cap);
-    } else {
-        cudaError_t e = cudaFuncSetAttribute(mxk_ksplit_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem_bytes(0, FieldGeom<0>::kSeg));
-        if (e != cudaSuccess) return e;
-        mxk_ksplit_kernel<0><<<grid, kThreads, smem, stream>>>(T, status, seg_cap);
-    }
-    return cudaGetLastError();
+    if (gf16) return launch_ksplit_impl<1>(T, status, stream);
+    return launch_ksplit_impl<0>(T, status, stream);
 }
 
 cudaError_t launch_wait_selftest(int32_t* status, uint64_t limit_ns, cudaStream_t stream) {
