@@ -376,12 +376,14 @@ int grid_for(uint64_t items, int threads) {
 // Full transform of 2^D bit-sliced rows (heap root 1), forward or inverse.
 cudaError_t run_transform(uint8_t* work, uint32_t G, int D, const uint16_t* factors, bool forward,
                           cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
+    static uint64_t attr = 0;
+    if (first_on_device(attr)) {
         cudaError_t e = cudaFuncSetAttribute(afft_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              kTileBytes);
-        if (e != cudaSuccess) return e;
-        attr = true;
+        if (e != cudaSuccess) {
+            attr = 0;
+            return e;
+        }
     }
     const uint32_t gt = std::min<uint32_t>(G, 16);
     int cmax = 1;
@@ -416,12 +418,14 @@ uint32_t mod_pow(uint32_t base, uint32_t e) {
 }
 
 cudaError_t run_wht(uint32_t* v, uint32_t ts, int D, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
+    static uint64_t attr = 0;
+    if (first_on_device(attr)) {
         cudaError_t e = cudaFuncSetAttribute(wht_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              8192 * 4);
-        if (e != cudaSuccess) return e;
-        attr = true;
+        if (e != cudaSuccess) {
+            attr = 0;
+            return e;
+        }
     }
     // passes of at most 8 index bits: enough groups per pass to spread over
     // the SMs (one CTA per group of 2^nb elements)

@@ -7,6 +7,18 @@
 
 namespace scrs {
 
+// Per-device one-time set-up flags (function attributes such as the dynamic
+// shared-memory limit are set per device): true the first time it is called
+// for the current device, false afterwards.
+inline bool first_on_device(uint64_t& done_mask) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return true;
+    const uint64_t bit = 1ull << dev;
+    if (done_mask & bit) return false;
+    done_mask |= bit;
+    return true;
+}
+
 constexpr uint16_t kNoRow = 0xFFFFu;
 constexpr int kThreads = 128;   // 4 warps per CTA
 constexpr int kMaxOutGroup = 64; // outputs computed per pass over the inputs

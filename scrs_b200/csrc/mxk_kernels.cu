@@ -757,13 +757,15 @@ size_t smem_bytes(int gf16, int max_in) {
 template <int kGf16>
 cudaError_t set_mxk_attrs() {
     using G = FieldGeom<kGf16>;
-    static bool done = false;
-    if (done) return cudaSuccess;
+    static uint64_t done = 0;
+    if (!first_on_device(done)) return cudaSuccess;
     const int smem = (int)smem_bytes(kGf16, G::kSeg);
     cudaError_t e = cudaFuncSetAttribute(mxk_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(mxk_single_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e == cudaSuccess) done = true;
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(mxk_ksplit_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) done = 0;
     return e;
 }
 
@@ -772,13 +774,8 @@ cudaError_t set_mxk_attrs() {
 template <int kGf16>
 cudaError_t launch_ksplit_impl(const MxkTask& T, int32_t* status, cudaStream_t stream) {
     using G = FieldGeom<kGf16>;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(mxk_ksplit_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem_bytes(kGf16, G::kSeg));
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    cudaError_t ea = set_mxk_attrs<kGf16>();
+    if (ea != cudaSuccess) return ea;
     if (!T.accumulate && T.n_out) {
         const uint64_t words = (uint64_t)T.n_out * (T.L / 4);
         zero_out_rows_kernel<<<(int)std::min<uint64_t>((words + 255) / 256, 148 * 16), 256, 0, stream>>>(T);
