@@ -388,9 +388,13 @@ cudaError_t run_transform(uint8_t* work, uint32_t G, int D, const uint16_t* fact
     const uint32_t gt = std::min<uint32_t>(G, 16);
     int cmax = 1;
     while (cmax < D && ((size_t)2 << cmax) * gt * 64 <= (size_t)kTileBytes) cmax++;
+    // the fewest passes the tile size allows, with levels spread evenly over
+    // them: smaller tiles for the same traffic, so more CTAs per pass
+    const int n_pass = (D + cmax - 1) / cmax;
+    const int cbal = (D + n_pass - 1) / n_pass;
     std::vector<std::pair<int, int>> passes;  // (l0, c) top-down
     for (int l0 = 0; l0 < D;) {
-        int c = std::min(cmax, D - l0);
+        int c = std::min(cbal, D - l0);
         passes.push_back({l0, c});
         l0 += c;
     }
