@@ -91,33 +91,6 @@ __device__ __forceinline__ void bitslice_lane(typename Lane<kGf16>::Words& w) {
     }
 }
 
-template <int kGf16>
-__device__ __forceinline__ void mul_planes(uint32_t c, typename Lane<kGf16>::Words& acc,
-                                           const typename Lane<kGf16>::Words& p) {
-    if constexpr (kGf16) {
-        mul16<true>(c, acc, p);
-    } else {
-        mul8x2_dispatch<true>(c, acc, p);  // the same coefficient on both plane sets
-    }
-}
-
-template <int kGf16>
-__device__ __forceinline__ void load_lane(const uint8_t* base, int lane, typename Lane<kGf16>::Words& w) {
-#pragma unroll
-    for (int pc = 0; pc < Lane<kGf16>::kPieces; pc++) {
-        uint4 v = *reinterpret_cast<const uint4*>(base + piece_pos(pc, lane));
-        w[4 * pc] = v.x, w[4 * pc + 1] = v.y, w[4 * pc + 2] = v.z, w[4 * pc + 3] = v.w;
-    }
-}
-
-template <int kGf16>
-__device__ __forceinline__ void store_lane(uint8_t* base, int lane, const typename Lane<kGf16>::Words& w) {
-#pragma unroll
-    for (int pc = 0; pc < Lane<kGf16>::kPieces; pc++)
-        *reinterpret_cast<uint4*>(base + piece_pos(pc, lane)) =
-            make_uint4(w[4 * pc], w[4 * pc + 1], w[4 * pc + 2], w[4 * pc + 3]);
-}
-
 // Issue the TMA copies of input rows [seg, seg + seg_n) of one chunk.  Called
 // by all 32 lanes of one warp: lane i < seg_n resolves and copies row seg + i,
 // so the row-number loads overlap instead of following one another.
