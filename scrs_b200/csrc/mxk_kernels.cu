@@ -29,7 +29,7 @@ namespace {
 // Shared-memory header: mbarrier (0), item words (8, 12), task descriptor
 // (16), one step list per warp (kStepOffset).
 constexpr int kStepOffset = 128;
-constexpr int kStepBytes = 144;  // u16 steps: 4 * kSeg + fold marker + 1 read-ahead
+constexpr int kStepBytes = 144;  // u16 steps: 4 * kSeg + 1 read-ahead
 constexpr int kSmemHeader = kStepOffset + 4 * kStepBytes;
 static_assert(2 * (4 * FieldGeom<1>::kSeg + 2) <= kStepBytes, "step list too short");
 static_assert(FieldGeom<0>::kSeg <= 32 && FieldGeom<1>::kSeg <= 32, "one lane per staged row");
@@ -174,8 +174,8 @@ __device__ __forceinline__ void load_out_planes(const uint8_t* orow, uint64_t of
 // step from a single jump site, so it stays in the SM's instruction cache; a
 // 256-way or two 16-way tables do not, and their misses cost more than the
 // second pass over the staged rows.  The warp runs a step list of
-// (i << 5) | (u-flag << 4) | nibble entries: the high-nibble pass, a fold
-// marker 0, then the low-nibble pass.
+// (i * chunk bytes) | (u-flag << 4) | nibble entries: the high-nibble pass,
+// the x16 fold, then the low-nibble pass.
 template <int kGf16>
 __device__ __forceinline__ void output_row(const uint8_t* buf, uint32_t c, uint16_t* steps, uint32_t seg_n, int lane,
                                            bool existing, uint8_t* orow, uint64_t off, uint64_t L, bool aligned,
@@ -188,28 +188,46 @@ __device__ __forceinline__ void output_row(const uint8_t* buf, uint32_t c, uint1
     // nibbles of the x-term (c0, or the GF(256) coefficient) and the u-term (c1)
     const uint32_t cx = c & 0xFFu, cu = kGf16 ? (c >> 8) & 0xFFu : 0u;
     const uint32_t below = (1u << lane) - 1u;
-    uint32_t n_steps = 0;
+    // step entries: (i * chunk bytes) | (u-flag << 4) | nibble; pass 0 (high
+    // nibbles) is entries [0, n0), pass 1 (low nibbles) [n0, n_steps)
+    static_assert(G::kChunk == 2048 && G::kSeg <= 16, "step entries hold i * 2048 in 16 bits");
+    uint32_t n0 = 0, n_steps = 0;
 #pragma unroll
     for (int pass = 0; pass < 2; pass++) {
         const uint32_t vx = pass ? cx & 15u : cx >> 4, vu = pass ? cu & 15u : cu >> 4;
         const uint32_t mx = __ballot_sync(0xFFFFFFFFu, vx != 0), mu = __ballot_sync(0xFFFFFFFFu, vu != 0);
         const uint32_t at = n_steps + __popc(mx & below) + __popc(mu & below);
-        if (vx) steps[at] = (uint16_t)((lane << 5) | vx);
-        if (vu) steps[at + (vx != 0)] = (uint16_t)((lane << 5) | 16u | vu);
+        const uint32_t row = (uint32_t)lane * G::kChunk;
+        if (vx) steps[at] = (uint16_t)(row | vx);
+        if (vu) steps[at + (vx != 0)] = (uint16_t)(row | 16u | vu);
         n_steps += __popc(mx) + __popc(mu);
-        if (pass == 0) {
-            if (lane == 0) steps[n_steps] = 0;  // fold marker
-            n_steps++;
-        }
+        if (pass == 0) n0 = n_steps;
     }
     __syncwarp();
 #pragma unroll
     for (int t = 0; t < kWords; t++) acc[t] = 0;
     const uint8_t* lane_buf = buf + 16 * lane;
+    uint32_t s = 0;
     uint32_t d = steps[0];
-    for (uint32_t s = 0; s < n_steps; s++) {
-        const uint32_t dn = steps[s + 1];
-        if (d == 0) {  // high nibbles done: acc = 16 * acc, plus the existing content
+#pragma unroll 1
+    for (int pass = 0; pass < 2; pass++) {  // one loop body, so one jump site
+        const uint32_t end = pass ? n_steps : n0;
+        for (; s < end; s++) {
+            const uint32_t dn = steps[s + 1];
+            Words p;
+            const uint8_t* src = lane_buf + (d & ~31u);
+#pragma unroll
+            for (int pc = 0; pc < 4; pc++) {
+                const uint4 v = *reinterpret_cast<const uint4*>(src + pc * 512);
+                p[4 * pc] = v.x, p[4 * pc + 1] = v.y, p[4 * pc + 2] = v.z, p[4 * pc + 3] = v.w;
+            }
+            if (kGf16 && (d & 16u)) mul_by_u(p);
+#if defined(__CUDA_ARCH__)
+            brx_mul8x2_lo(d & 15u, acc, p);
+#endif
+            d = dn;
+        }
+        if (pass == 0) {  // high nibbles done: acc = 16 * acc, plus the existing content
 #pragma unroll
             for (int h = 0; h < kWords; h += 8) {
                 uint32_t t16[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -223,20 +241,7 @@ __device__ __forceinline__ void output_row(const uint8_t* buf, uint32_t c, uint1
 #pragma unroll
                 for (int t = 0; t < kWords; t++) acc[t] ^= e[t];
             }
-        } else {
-            Words p;
-            const uint8_t* src = lane_buf + (d >> 5) * (uint32_t)G::kChunk;
-#pragma unroll
-            for (int pc = 0; pc < 4; pc++) {
-                const uint4 v = *reinterpret_cast<const uint4*>(src + pc * 512);
-                p[4 * pc] = v.x, p[4 * pc + 1] = v.y, p[4 * pc + 2] = v.z, p[4 * pc + 3] = v.w;
-            }
-            if (kGf16 && (d & 16u)) mul_by_u(p);
-#if defined(__CUDA_ARCH__)
-            brx_mul8x2_lo(d & 15u, acc, p);
-#endif
         }
-        d = dn;
     }
     __syncwarp();  // the list is rebuilt for the warp's next output row
     bitslice_lane<kGf16>(acc);
