@@ -46,9 +46,17 @@ METRIC = "encode/decode GB/s and HBM-roofline % on 1 B200; batched vs plain; p50
 K, M, L = 10, 4, 4096
 STRIPES = 65536
 SEED = 0x5C250001
-WORKLOAD = ("GF(256) Good Cauchy k=10 m=4 symbol_len=4096: 65536 stripes encoded + 65536 stripes "
-            "batch-decoded from seeded random 10-of-14 symbol sets, per GPU per step, one persistent "
+
+
+def workload() -> str:
+    return (f"GF(256) Good Cauchy k={K} m={M} symbol_len={L}: {STRIPES} stripes encoded + {STRIPES} stripes "
+            f"batch-decoded from seeded random {K}-of-{K + M} symbol sets, per GPU per step, one persistent "
             "launch (CUDA graph)")
+
+
+def input_bytes() -> int:
+    """Device bytes read by one step: k data rows per encoded stripe, k received rows per decoded stripe."""
+    return 2 * STRIPES * K * L
 
 
 def peaks():
@@ -666,9 +674,11 @@ def run_ours(args, world, rank, local):
         "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8",
         "data": "synthetic: seeded uniform random bytes (torch.Generator), seeded 10-of-14 erasure sets",
-        "config": {"workload": WORKLOAD, "engine": "GoodCauchy", "k": K, "m": M, "symbol_len": L,
+        "config": {"workload": workload(), "engine": "GoodCauchy", "k": K, "m": M, "symbol_len": L,
                    "stripes_encode": STRIPES, "stripes_decode": STRIPES, "goodput_bytes_per_step": goodput_bytes(),
-                   "l2": "inputs 5.4 GB per GPU > 126 MB L2, no flush needed", "parallelism": f"weak x{world}",
+                   "l2": (f"inputs {input_bytes() / 1e9:.2f} GB per GPU > 126 MB L2, no flush needed"
+                          if input_bytes() > 126 << 20 else
+                          f"inputs {input_bytes() / 1e6:.1f} MB per GPU fit in the 126 MB L2 (small case)"), "parallelism": f"weak x{world}",
                    "bit_exact": ok},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk.result, "extras": extras,
@@ -699,7 +709,7 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic: seeded uniform random bytes",
-        "config": {"workload": WORKLOAD, "engine": "GoodCauchy", "k": K, "m": M, "symbol_len": L,
+        "config": {"workload": workload(), "engine": "GoodCauchy", "k": K, "m": M, "symbol_len": L,
                    "parallelism": f"weak x{world}"},
         "cpu_baseline": cpu, "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                                      "d2h_bytes_per_step": 0}}))
