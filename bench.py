@@ -341,6 +341,11 @@ def extra_mixed(torch, api):
                  outbuf.data_ptr() + out_off.astype(np.uint64), indices=idx)
     goodput = float((ks * Ls).sum())
     algo = float(np.where(op == OP_ENCODE, (ks + ms) * Ls, 2 * ks * Ls).sum())
+    default = b.launch_params
+    b.run(graph=True)
+    torch.cuda.synchronize()
+    t_default = time_ms(torch, lambda: b.run(graph=True), 10)
+    tuned = b.autotune(reps=3)  # the graph is re-captured with the tuned launch
     b.run(graph=True)
     torch.cuda.synchronize()
     t_graph = time_ms(torch, lambda: b.run(graph=True), 10)
@@ -357,6 +362,10 @@ def extra_mixed(torch, api):
             "speedup": round(t_plain / t_graph, 2),
             "persistent_ms": round(t_graph, 3), "plain_ms": round(t_plain, 3),
             "persistent_hbm_frac": round(algo / t_graph / 1e6 / peaks()[0], 3),
+            "autotune": {"default": {"seg_rows": default.seg_rows, "ctas_per_sm": default.ctas_per_sm,
+                                     "persistent_ms": round(t_default, 3)},
+                         "chosen": {"seg_rows": tuned.seg_rows, "ctas_per_sm": tuned.ctas_per_sm,
+                                    "persistent_ms": round(t_graph, 3)}},
             "launches": {"persistent": launches_batched, "plain": launches_plain}}
 
 
@@ -400,7 +409,7 @@ def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C25
     """Config 5: Poisson arrivals of mixed encode/decode requests over all four
     engines through the serving loop (scrs_server_*), 64 GB budget, 8 slots.
     The rate sweep is 0.25x, 0.5x and 0.75x the closed-loop capacity measured
-    first.  Payloads are seeded random device bytes (decode requests decode
+    first (median of three passes).  Payloads are seeded random device bytes (decode requests decode
     random received rows: the same work; bit-exactness is covered by the
     serving tests).  Latency = completion seen by the host - submit."""
     from scrs_b200.api import Engine
@@ -431,6 +440,7 @@ def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C25
             e = int(rng.integers(0, min(k, m) + 1))
             erased = set(rng.choice(k, e, replace=False).tolist()) if e else set()
             idx = [i for i in range(k) if i not in erased] + [k + j for j in rng.choice(m, e, replace=False).tolist()]
+            idx = np.asarray(idx, dtype=np.uint64)
         templates.append((op, engine, k, m, Ls, d_in, d_out, idx))
     srv = Server(api.lib, 64 << 30, slots=8)
 
@@ -444,18 +454,21 @@ def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C25
         for t in range(len(templates)):
             submit(t, t)
         srv.drain(600)
-    order = rng.integers(0, len(templates), 2000)
-    t0 = time.perf_counter()
-    for i, t in enumerate(order):
-        submit(int(t), int(t))
-    srv.drain(600)
-    cap_s = time.perf_counter() - t0
-    cap_rate = len(order) / cap_s
-    cap_bytes = sum(templates[int(t)][2] * templates[int(t)][4] for t in order)
+    passes = []  # closed loop: 3 passes of 2000 requests submitted at once, median kept
+    for _ in range(3):
+        order = rng.integers(0, len(templates), 2000)
+        t0 = time.perf_counter()
+        for t in order:
+            submit(int(t), int(t))
+        srv.drain(600)
+        cap_s = time.perf_counter() - t0
+        passes.append((len(order) / cap_s, sum(templates[int(t)][2] * templates[int(t)][4] for t in order) / cap_s))
+    cap_rate, cap_gbps = sorted(passes)[1]
     res = {"workload": "Poisson arrivals; 70% GF(256) (Standard/Good, k~U[4,64], m~U[1,16], L in {1,4,16,64} KiB), "
                        "15% tower (k<=1024, m<=256), 15% AFFT (k<=16384, m<=16384, L 256-2048); half encode, half "
                        "decode with random erasures <= m; 64 GB budget, 8 slots, GF(256) coalesced per slot",
-           "closed_loop": {"requests_per_s": round(cap_rate, 1), "goodput_GBps": round(cap_bytes / cap_s / 1e9, 2)},
+           "closed_loop": {"requests_per_s": round(cap_rate, 1), "goodput_GBps": round(cap_gbps / 1e9, 2),
+                           "passes_requests_per_s": [round(r, 1) for r, _ in passes]},
            "rates": []}
     for frac in (0.25, 0.5, 0.75):
         rate = frac * cap_rate
@@ -583,6 +596,7 @@ def run_ours(args, world, rank, local):
     api = scrs_b200.api_default()
     w = build_cfg1(torch, api, rank)
     b = w["batch"]
+    tuned = b.autotune(reps=3)  # launch parameters of the drain, chosen before any timing
     for _ in range(max(args.warmup, 3)):
         b.run(graph=True)
     torch.cuda.synchronize()
@@ -679,7 +693,9 @@ def run_ours(args, world, rank, local):
                    "l2": (f"inputs {input_bytes() / 1e9:.2f} GB per GPU > 126 MB L2, no flush needed"
                           if input_bytes() > 126 << 20 else
                           f"inputs {input_bytes() / 1e6:.1f} MB per GPU fit in the 126 MB L2 (small case)"), "parallelism": f"weak x{world}",
-                   "bit_exact": ok},
+                   "bit_exact": ok,
+                   "drain_launch": {"seg_rows": tuned.seg_rows, "ctas_per_sm": tuned.ctas_per_sm,
+                                    "chosen_by": "scrs_stripe_batch_autotune"}},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk.result, "extras": extras,
     }

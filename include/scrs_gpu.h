@@ -348,7 +348,9 @@ SCRS_API int32_t scrs_stripe_batch_set(scrs_stripe_batch* batch,
  * piece p+1 are copied in and the outputs of piece p-1 copied out (on two
  * internal streams) while piece p computes; the run's stream waits for the
  * last copy.  Copies of stripes that are contiguous in host memory are
- * merged.  use_graph is ignored in this mode. */
+ * merged; a merged copy the driver refuses (host buffers that touch but are
+ * separate allocations) is issued stripe by stripe instead.  use_graph is
+ * ignored in this mode. */
 SCRS_API int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* batch,
                                             const scrs_stripe_desc* descs,
                                             uint64_t count, scrs_error* err);
@@ -372,6 +374,60 @@ SCRS_API int32_t scrs_stripe_batch_run_timed(scrs_stripe_batch* batch, void* str
 /* After the run's stream has synchronised: SCRS_OK, or the device-side
  * failure a kernel recorded (SCRS_ERR_DEVICE_TIMEOUT). */
 SCRS_API int32_t scrs_stripe_batch_check(scrs_stripe_batch* batch, scrs_error* err);
+
+/* ---- Autotuner for the persistent drain ----------------------------------
+ * No reference counterpart.  Two launch parameters of the drain kernel are
+ * tuned per batch geometry:
+ *   seg_rows     input rows staged in shared memory per segment (1..32).
+ *                Stripes with more inputs than this pass over their output
+ *                rows once per segment; more rows cost shared memory per CTA
+ *                and so CTAs per SM.
+ *   ctas_per_sm  CTAs of the persistent grid per SM (with the SM count this
+ *                fixes the grid, hence the stripes each CTA drains).
+ * A process-wide table maps a geometry key to chosen parameters, and every
+ * scrs_stripe_batch_run consults it; a batch whose key has no entry stages
+ * min(largest k, 16) rows and runs the most CTAs per SM that fit.  Changing
+ * the table re-captures graphs on their next run. */
+typedef struct scrs_tune_key {
+    uint32_t field;    /* 0: GF(256) stripe batches                          */
+    uint32_t k_bucket; /* ceil(log2(largest k))                              */
+    uint32_t m_bucket; /* ceil(log2(mean output rows per stripe)), 0 if <= 1 */
+    uint32_t l_bucket; /* floor(log2(mean symbol_len))                       */
+} scrs_tune_key;
+
+typedef struct scrs_tune_params {
+    uint32_t seg_rows;    /* 1..32                                          */
+    uint32_t ctas_per_sm; /* 1..32; capped by what fits at run time         */
+    float drain_ms;       /* the winner's measured drain time (informative) */
+    uint32_t reserved;
+} scrs_tune_params;
+
+/* Key of a descriptor list (host only; no device work). */
+SCRS_API int32_t scrs_tune_key_of(const scrs_stripe_desc* descs, uint64_t count,
+                                  scrs_tune_key* key, scrs_error* err);
+/* Key of the batch's current descriptors. */
+SCRS_API int32_t scrs_stripe_batch_tune_key(const scrs_stripe_batch* batch, scrs_tune_key* key,
+                                            scrs_error* err);
+/* The seg_rows and ctas_per_sm a run of the batch would use now. */
+SCRS_API int32_t scrs_stripe_batch_launch_params(const scrs_stripe_batch* batch,
+                                                 scrs_tune_params* params, scrs_error* err);
+/* Time the drain of the batch's current stripes on `stream` under each
+ * candidate (seg_rows in {8, 12, 16, 24, 32, largest k} capped at the
+ * largest k; ctas_per_sm in {most that fit, 3/4 of it, 1/2 of it}), one
+ * untimed and `reps` timed launches each (0 means 5, at most 100), keep the
+ * fastest median (the default must be beaten by 1 %), store it in the table
+ * under the batch's key and return it.  Outputs are rewritten with the same
+ * values by every launch; a host-buffer batch first runs once to stage its
+ * inputs.  Synchronises `stream`. */
+SCRS_API int32_t scrs_stripe_batch_autotune(scrs_stripe_batch* batch, void* stream, uint32_t reps,
+                                            scrs_tune_params* chosen, scrs_error* err);
+/* The table (for saving and loading it): entries 0..size-1, set, clear. */
+SCRS_API uint64_t scrs_tune_table_size(void);
+SCRS_API int32_t scrs_tune_table_entry(uint64_t i, scrs_tune_key* key, scrs_tune_params* params,
+                                       scrs_error* err);
+SCRS_API int32_t scrs_tune_table_set(const scrs_tune_key* key, const scrs_tune_params* params,
+                                     scrs_error* err);
+SCRS_API void scrs_tune_table_clear(void);
 
 /* ---- Serving loop (continuous batching) ----------------------------------
  * No reference counterpart: a request loop over the engines above.  Requests

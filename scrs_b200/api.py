@@ -83,7 +83,7 @@ _STATUS = {
     307: ("DecodeError", "WrongOutputLen", ("expected", "got")),
     308: ("DecodeError", "ScratchMismatch", ()),
     901: ("RuntimeFailure", "NullArgument", ()),
-    902: ("RuntimeFailure", "Cuda", ("cuda_error",)),
+    902: ("RuntimeFailure", "Cuda", ("cuda_error", "source_line")),
     903: ("RuntimeFailure", "OutOfMemory", ("bytes",)),
     904: ("RuntimeFailure", "NoDevice", ()),
     905: ("RuntimeFailure", "Capacity", ("requested", "limit")),

@@ -148,3 +148,34 @@ class StripeBatch:
     @property
     def last_launches(self) -> int:
         return int(self._lib.lib.scrs_stripe_batch_last_launches(self._ptr))
+
+    def autotune(self, reps: int = 5, stream=None):
+        """Time the drain's launch candidates on this batch's stripes, store the
+        fastest in the library's tuning table under the batch's geometry key
+        and return it (``tune.TuneParams``)."""
+        from . import tune
+
+        tune.bind(self._lib)
+        p, err = tune._Params(), _Error()
+        self._lib.check(self._lib.lib.scrs_stripe_batch_autotune(self._ptr, _stream_ptr(stream), reps, C.byref(p),
+                                                                 C.byref(err)), err)
+        return tune._params(p)
+
+    @property
+    def launch_params(self):
+        """The seg_rows / ctas_per_sm a run would use now (``tune.TuneParams``)."""
+        from . import tune
+
+        tune.bind(self._lib)
+        p, err = tune._Params(), _Error()
+        self._lib.check(self._lib.lib.scrs_stripe_batch_launch_params(self._ptr, C.byref(p), C.byref(err)), err)
+        return tune._params(p)
+
+    @property
+    def tune_key(self):
+        from . import tune
+
+        tune.bind(self._lib)
+        k, err = tune._Key(), _Error()
+        self._lib.check(self._lib.lib.scrs_stripe_batch_tune_key(self._ptr, C.byref(k), C.byref(err)), err)
+        return tune._key(k)

@@ -15,7 +15,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 OUT = HERE / "_lib" / "libscrs_b200.so"
-SOURCES = ["mxk_kernels.cu", "afft.cu", "engines.cu", "batch.cu", "noalloc.cu", "server.cu"]
+SOURCES = ["mxk_kernels.cu", "afft.cu", "engines.cu", "batch.cu", "noalloc.cu", "server.cu", "tune.cu"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-gencode", "arch=compute_100a,code=sm_100a",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
 

@@ -23,6 +23,7 @@
 
 #include "host_field.h"
 #include "runtime.h"
+#include "tune.h"
 
 using namespace scrs;
 
@@ -35,7 +36,9 @@ struct scrs_stripe_batch {
     std::vector<CauchyPlanTask> plans;
     std::vector<uint8_t> arena;
     uint32_t total_items = 0, max_in = 1, max_plan_r = 0;
+    scrs_tune_key key{};  // geometry key of the current descriptors (autotuner table)
     cudaGraphExec_t graph = nullptr;
+    uint64_t graph_version = 0;   // autotuner table version the graph was captured under
     uint64_t graph_launches = 0;  // kernels in the captured graph
     uint64_t last_launches = 0;
     int sm_count = 0;
@@ -46,6 +49,8 @@ struct scrs_stripe_batch {
         const void* src;
         void* dst;
         size_t bytes;
+        uint32_t part_lo, part_hi;  // the stripes' own copies this one merges
+        bool split;                 // the driver refused the merged form
     };
     struct Piece {
         uint32_t item_lo, item_hi, plan_lo, plan_hi;
@@ -53,7 +58,8 @@ struct scrs_stripe_batch {
     };
     bool host_mode = false;
     DevBuf stage_in, stage_out;
-    std::vector<Copy> h2d, d2h;
+    std::vector<Copy> h2d, d2h;              // merged copies
+    std::vector<Copy> h2d_parts, d2h_parts;  // one per stripe
     std::vector<Piece> pieces;
     cudaStream_t s_in = nullptr, s_out = nullptr;
     std::vector<cudaEvent_t> events;  // start, end, then per piece: copied in, computed
@@ -240,6 +246,7 @@ int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc
     b->plan_begin[count] = (uint32_t)b->plans.size();
     b->total_items = item;
     b->max_in = max_in;
+    b->key = tune_key_of(descs, count);
     b->item_task.resize(item);
     for (size_t t = 0; t < b->tasks.size(); t++)
         std::fill(b->item_task.begin() + b->tasks[t].item_begin,
@@ -294,6 +301,8 @@ extern "C" int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* b, const scrs_s
     std::vector<scrs_stripe_desc> dev(descs, descs + count);
     b->h2d.clear();
     b->d2h.clear();
+    b->h2d_parts.clear();
+    b->d2h_parts.clear();
     // piece boundaries: about equal input bytes per piece
     const size_t n_pieces = std::min<size_t>(kMaxPieces, std::max<uint64_t>(count, 1));
     std::vector<uint64_t> cut;  // first stripe of each piece, then count
@@ -321,17 +330,26 @@ extern "C" int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* b, const scrs_s
         uint8_t* dout = b->stage_out.as<uint8_t>() + oo;
         dev[s].in = din;
         dev[s].out = dout;
-        // merge with the previous copy of the same piece when both sides are contiguous
+        // merge with the previous copy of the same piece when both sides are
+        // contiguous (the stripe's own copy is kept in case the driver refuses
+        // a merged copy whose host side spans two allocations)
+        const uint32_t part = (uint32_t)b->h2d_parts.size();
+        b->h2d_parts.push_back({d.in, din, ib, part, part + 1, false});
+        b->d2h_parts.push_back({dout, d.out, ob, part, part + 1, false});
         if (!first && (const uint8_t*)b->h2d.back().src + b->h2d.back().bytes == d.in &&
-            (uint8_t*)b->h2d.back().dst + b->h2d.back().bytes == din)
+            (uint8_t*)b->h2d.back().dst + b->h2d.back().bytes == din) {
             b->h2d.back().bytes += ib;
-        else
-            b->h2d.push_back({d.in, din, ib});
+            b->h2d.back().part_hi = part + 1;
+        } else {
+            b->h2d.push_back({d.in, din, ib, part, part + 1, false});
+        }
         if (!first && (const uint8_t*)b->d2h.back().src + b->d2h.back().bytes == dout &&
-            (uint8_t*)b->d2h.back().dst + b->d2h.back().bytes == d.out)
+            (uint8_t*)b->d2h.back().dst + b->d2h.back().bytes == d.out) {
             b->d2h.back().bytes += ob;
-        else
-            b->d2h.push_back({dout, d.out, ob});
+            b->d2h.back().part_hi = part + 1;
+        } else {
+            b->d2h.push_back({dout, d.out, ob, part, part + 1, false});
+        }
         oi += (ib + 15) & ~(size_t)15;
         oo += (ob + 15) & ~(size_t)15;
         if (s + 1 == cut[piece + 1]) piece++;
@@ -365,16 +383,59 @@ extern "C" int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* b, const scrs_s
 
 namespace {
 
+// Enqueue merged copy `c` on `st`.  Host buffers of consecutive stripes may
+// touch without being one allocation; the driver refuses a copy spanning
+// two (cudaErrorInvalidValue, nothing enqueued), and such a copy is split
+// into its stripes' own copies, now and on every later run.
+int32_t issue_copy(scrs_stripe_batch::Copy& c, const std::vector<scrs_stripe_batch::Copy>& parts,
+                   cudaMemcpyKind kind, cudaStream_t st, scrs_error* err) {
+    if (!c.split) {
+        const cudaError_t e = cudaMemcpyAsync(c.dst, c.src, c.bytes, kind, st);
+        if (e == cudaSuccess) return SCRS_OK;
+        if (e != cudaErrorInvalidValue || c.part_hi - c.part_lo < 2) return set_err(err, SCRS_ERR_CUDA, e, __LINE__);
+        cudaGetLastError();
+        c.split = true;
+    }
+    for (uint32_t q = c.part_lo; q < c.part_hi; q++)
+        SCRS_CUDA(cudaMemcpyAsync(parts[q].dst, parts[q].src, parts[q].bytes, kind, st));
+    return SCRS_OK;
+}
+
 int32_t copy_in(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
     if (!b->host_mode) return SCRS_OK;
-    for (auto& c : b->h2d) SCRS_CUDA(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, st));
+    for (auto& c : b->h2d) {
+        int32_t r = issue_copy(c, b->h2d_parts, cudaMemcpyHostToDevice, st, err);
+        if (r) return r;
+    }
     return SCRS_OK;
 }
 
 int32_t copy_out(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
     if (!b->host_mode) return SCRS_OK;
-    for (auto& c : b->d2h) SCRS_CUDA(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, st));
+    for (auto& c : b->d2h) {
+        int32_t r = issue_copy(c, b->d2h_parts, cudaMemcpyDeviceToHost, st, err);
+        if (r) return r;
+    }
     return SCRS_OK;
+}
+
+// Drain launch parameters: the autotuner's entry for the batch's key, else
+// min(largest k, 16) rows per segment and the most CTAs per SM that fit.
+struct DrainCfg {
+    int seg_rows, ctas_per_sm, grid;
+};
+
+DrainCfg drain_cfg(const scrs_stripe_batch* b) {
+    DrainCfg c{mxk_default_seg((int)b->max_in), 0, 0};
+    scrs_tune_params p{};
+    if (tune_lookup(b->key, &p)) {
+        c.seg_rows = std::max(1, std::min({(int)p.seg_rows, (int)b->max_in, FieldGeom<0>::kSegMax}));
+        c.ctas_per_sm = (int)p.ctas_per_sm;
+    }
+    const int fit = mxk_ctas_per_sm(c.seg_rows);
+    if (c.ctas_per_sm <= 0 || c.ctas_per_sm > fit) c.ctas_per_sm = fit;
+    c.grid = std::max(1, std::min<int>(b->sm_count * c.ctas_per_sm, (int)std::max<uint32_t>(b->total_items, 1)));
+    return c;
 }
 
 int32_t enqueue_batch(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
@@ -385,10 +446,9 @@ int32_t enqueue_batch(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
         b->last_launches++;
     }
     if (b->total_items) {
-        int grid = b->sm_count * mxk_ctas_per_sm(0, (int)b->max_in);
-        grid = std::min<int>(grid, (int)b->total_items);
+        const DrainCfg c = drain_cfg(b);
         SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), 0, b->total_items,
-                                   b->d_counter.as<uint32_t>(), b->status.dev, (int)b->max_in, grid, st));
+                                   b->d_counter.as<uint32_t>(), b->status.dev, c.seg_rows, c.grid, st));
         b->last_launches++;
     }
     return SCRS_OK;
@@ -401,13 +461,15 @@ int32_t run_host(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
     SCRS_CUDA(cudaStreamWaitEvent(b->s_in, ev_start, 0));
     SCRS_CUDA(cudaStreamWaitEvent(b->s_out, ev_start, 0));
     SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, kMaxPieces * sizeof(uint32_t), st));
-    const int grid = b->sm_count * mxk_ctas_per_sm(0, (int)b->max_in);
+    const DrainCfg c = drain_cfg(b);
     b->last_launches = 0;
     for (size_t q = 0; q < b->pieces.size(); q++) {
         const scrs_stripe_batch::Piece& P = b->pieces[q];
         cudaEvent_t ev_in = b->events[2 + 2 * q], ev_done = b->events[3 + 2 * q];
-        for (size_t c = P.h2d_lo; c < P.h2d_hi; c++)
-            SCRS_CUDA(cudaMemcpyAsync(b->h2d[c].dst, b->h2d[c].src, b->h2d[c].bytes, cudaMemcpyHostToDevice, b->s_in));
+        for (size_t i = P.h2d_lo; i < P.h2d_hi; i++) {
+            int32_t r = issue_copy(b->h2d[i], b->h2d_parts, cudaMemcpyHostToDevice, b->s_in, err);
+            if (r) return r;
+        }
         SCRS_CUDA(cudaEventRecord(ev_in, b->s_in));
         SCRS_CUDA(cudaStreamWaitEvent(st, ev_in, 0));
         if (P.plan_hi > P.plan_lo) {
@@ -417,13 +479,15 @@ int32_t run_host(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
         }
         if (P.item_hi > P.item_lo) {
             SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), P.item_lo, P.item_hi,
-                                       b->d_counter.as<uint32_t>() + q, b->status.dev, (int)b->max_in, grid, st));
+                                       b->d_counter.as<uint32_t>() + q, b->status.dev, c.seg_rows, c.grid, st));
             b->last_launches++;
         }
         SCRS_CUDA(cudaEventRecord(ev_done, st));
         SCRS_CUDA(cudaStreamWaitEvent(b->s_out, ev_done, 0));
-        for (size_t c = P.d2h_lo; c < P.d2h_hi; c++)
-            SCRS_CUDA(cudaMemcpyAsync(b->d2h[c].dst, b->d2h[c].src, b->d2h[c].bytes, cudaMemcpyDeviceToHost, b->s_out));
+        for (size_t i = P.d2h_lo; i < P.d2h_hi; i++) {
+            int32_t r = issue_copy(b->d2h[i], b->d2h_parts, cudaMemcpyDeviceToHost, b->s_out, err);
+            if (r) return r;
+        }
     }
     SCRS_CUDA(cudaEventRecord(ev_end, b->s_out));
     SCRS_CUDA(cudaStreamWaitEvent(st, ev_end, 0));
@@ -445,6 +509,10 @@ extern "C" int32_t scrs_stripe_batch_run(scrs_stripe_batch* b, void* stream, int
         if (r) return r;
         return set_err(err, SCRS_OK);
     }
+    if (b->graph && b->graph_version != tune_version()) {  // launch parameters may have changed
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
     if (!b->graph) {
         // Capture on a private stream so the legacy default stream can be used by callers.
         cudaStream_t cap;
@@ -463,6 +531,7 @@ extern "C" int32_t scrs_stripe_batch_run(scrs_stripe_batch* b, void* stream, int
         }
         SCRS_CUDA(e);
         b->graph_launches = b->last_launches;
+        b->graph_version = tune_version();
         e = cudaGraphInstantiate(&b->graph, g, 0);
         cudaGraphDestroy(g);
         SCRS_CUDA(e);
@@ -509,9 +578,9 @@ extern "C" int32_t scrs_stripe_batch_run_timed(scrs_stripe_batch* b, void* strea
     }
     cudaEventRecord(ev[1], st);
     if (b->total_items) {
-        int grid = std::min<int>(b->sm_count * mxk_ctas_per_sm(0, (int)b->max_in), (int)b->total_items);
+        const DrainCfg c = drain_cfg(b);
         SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), 0, b->total_items,
-                                   b->d_counter.as<uint32_t>(), b->status.dev, (int)b->max_in, grid, st));
+                                   b->d_counter.as<uint32_t>(), b->status.dev, c.seg_rows, c.grid, st));
         b->last_launches++;
     }
     cudaEventRecord(ev[2], st);
@@ -529,5 +598,101 @@ extern "C" int32_t scrs_stripe_batch_check(scrs_stripe_batch* b, scrs_error* err
     if (!b) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
     int32_t r = take_status(b->status, err);
     if (r) return r;
+    return set_err(err, SCRS_OK);
+}
+
+extern "C" int32_t scrs_stripe_batch_tune_key(const scrs_stripe_batch* b, scrs_tune_key* key, scrs_error* err) {
+    if (!b || !key) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
+    *key = b->key;
+    return set_err(err, SCRS_OK);
+}
+
+extern "C" int32_t scrs_stripe_batch_launch_params(const scrs_stripe_batch* b, scrs_tune_params* params,
+                                                   scrs_error* err) {
+    if (!b || !params) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
+    const DrainCfg c = drain_cfg(b);
+    *params = scrs_tune_params{(uint32_t)c.seg_rows, (uint32_t)c.ctas_per_sm, 0.0f, 0};
+    return set_err(err, SCRS_OK);
+}
+
+namespace {
+
+// Median device time of `reps` drain launches (after one untimed launch).
+int32_t time_drain(scrs_stripe_batch* b, cudaStream_t st, int seg_rows, int grid, uint32_t reps, cudaEvent_t e0,
+                   cudaEvent_t e1, float* median_ms, scrs_error* err) {
+    std::vector<float> t;
+    for (uint32_t rep = 0; rep <= reps; rep++) {
+        SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, 4, st));
+        SCRS_CUDA(cudaEventRecord(e0, st));
+        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), 0, b->total_items,
+                                   b->d_counter.as<uint32_t>(), b->status.dev, seg_rows, grid, st));
+        SCRS_CUDA(cudaEventRecord(e1, st));
+        SCRS_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        SCRS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (rep) t.push_back(ms);
+    }
+    std::sort(t.begin(), t.end());
+    *median_ms = t[t.size() / 2];
+    return SCRS_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t scrs_stripe_batch_autotune(scrs_stripe_batch* b, void* stream, uint32_t reps,
+                                              scrs_tune_params* chosen, scrs_error* err) {
+    if (!b || !chosen) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
+    if (reps > 100) return set_err(err, SCRS_ERR_BAD_ARGUMENT, 3, reps);
+    if (reps == 0) reps = 5;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (b->total_items == 0) return scrs_stripe_batch_launch_params(b, chosen, err);
+    // inputs on the device and decode matrices built before any drain
+    if (b->host_mode) {
+        int32_t r = run_host(b, st, err);
+        if (r) return r;
+    } else if (!b->plans.empty()) {
+        SCRS_CUDA(launch_cauchy_plan(b->d_plans.as<CauchyPlanTask>(), (uint32_t)b->plans.size(), 0, b->max_plan_r, st));
+    }
+    const int max_seg = std::min<int>((int)b->max_in, FieldGeom<0>::kSegMax);
+    const int def_seg = mxk_default_seg((int)b->max_in);
+    std::vector<int> segs{def_seg};
+    for (int s : {8, 12, 16, 24, 32, max_seg}) {
+        s = std::min(s, max_seg);
+        if (std::find(segs.begin(), segs.end(), s) == segs.end()) segs.push_back(s);
+    }
+    cudaEvent_t e0, e1;
+    SCRS_CUDA(cudaEventCreate(&e0));
+    SCRS_CUDA(cudaEventCreate(&e1));
+    scrs_tune_params best{};
+    int32_t rc = SCRS_OK;
+    for (int seg : segs) {
+        const int fit = mxk_ctas_per_sm(seg);
+        std::vector<int> ctas{fit};
+        for (int c : {(3 * fit + 3) / 4, (fit + 1) / 2}) {
+            c = std::max(1, c);
+            if (std::find(ctas.begin(), ctas.end(), c) == ctas.end()) ctas.push_back(c);
+        }
+        for (int c : ctas) {
+            const int grid = std::max(1, std::min<int>(b->sm_count * c, (int)b->total_items));
+            float ms = 0;
+            rc = time_drain(b, st, seg, grid, reps, e0, e1, &ms, err);
+            if (rc) break;
+            // the default (first candidate) holds unless beaten by 1 %
+            if (best.seg_rows == 0 || ms < 0.99f * best.drain_ms)
+                best = scrs_tune_params{(uint32_t)seg, (uint32_t)c, ms, 0};
+        }
+        if (rc) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    rc = take_status(b->status, err);  // a drain that gave up on a wait
+    if (rc) return rc;
+    tune_store(b->key, best);
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    *chosen = best;
     return set_err(err, SCRS_OK);
 }

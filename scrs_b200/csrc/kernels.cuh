@@ -30,7 +30,8 @@ struct FieldGeom {
     static constexpr int kLaneBytes = 64;
     static constexpr int kChunk = 32 * kLaneBytes;     // bytes per row per CTA
     static constexpr int kPieces = kLaneBytes / 16;    // 16-byte pieces per lane
-    static constexpr int kSeg = 16;                    // input rows staged per segment
+    static constexpr int kSeg = 16;                    // input rows staged per segment (default)
+    static constexpr int kSegMax = kGf16 ? 16 : 32;    // most rows a segment may stage
     static constexpr int kElem = kGf16 ? 2 : 1;        // coefficient bytes
 };
 
@@ -81,10 +82,9 @@ struct CauchyPlanTask {
 // tasks[item_task[i]] (row chunk i - item_begin of that task).  work_counter
 // (zeroed before the launch) hands items out dynamically; nullptr strides
 // items by grid instead.
+// seg_rows: input rows staged per segment, 1..FieldGeom<0>::kSegMax.
 cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
-                             uint32_t* work_counter, int32_t* status, int max_in, int grid, cudaStream_t stream);
-cudaError_t launch_gf16_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
-                            uint32_t* work_counter, int32_t* status, int max_in, int grid, cudaStream_t stream);
+                             uint32_t* work_counter, int32_t* status, int seg_rows, int grid, cudaStream_t stream);
 // One task by value; grid <= 0 means one CTA per row chunk (or the
 // input-split form for more than one segment of inputs, see below).
 cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream);
@@ -101,9 +101,10 @@ cudaError_t launch_cauchy_plan(const CauchyPlanTask* tasks, uint32_t n_tasks, in
                                cudaStream_t stream);
 // Largest r the plan kernel keeps in shared memory.
 constexpr uint32_t kPlanSmemMaxR = 12288;
-// Shared-memory bytes a launch with this many input rows needs.
-size_t mxk_smem_bytes(int gf16, int max_in);
-// CTAs per SM the persistent launch uses for this shared-memory size.
-int mxk_ctas_per_sm(int gf16, int max_in);
+// Input rows per segment when nothing else is chosen: all of them up to kSeg.
+int mxk_default_seg(int max_in);
+// Most CTAs of the GF(256) persistent drain one SM holds with seg_rows rows
+// staged per segment (shared memory and registers permitting).
+int mxk_ctas_per_sm(int seg_rows);
 
 }  // namespace scrs

@@ -29,10 +29,12 @@ namespace {
 // Shared-memory header: mbarrier (0), item words (8, 12), task descriptor
 // (16), one step list per warp (kStepOffset).
 constexpr int kStepOffset = 128;
-constexpr int kStepBytes = 144;  // u16 steps: 4 * kSeg + 1 read-ahead
+constexpr int kStepBytes = 144;  // u16 steps, 2 per GF(256) or 4 per GF(2^16) input, + 1 read-ahead
 constexpr int kSmemHeader = kStepOffset + 4 * kStepBytes;
-static_assert(2 * (4 * FieldGeom<1>::kSeg + 2) <= kStepBytes, "step list too short");
-static_assert(FieldGeom<0>::kSeg <= 32 && FieldGeom<1>::kSeg <= 32, "one lane per staged row");
+// step entries: 2 per GF(256) input, 4 per GF(2^16) input, plus the read-ahead
+static_assert(2 * (4 * FieldGeom<1>::kSegMax + 1) <= kStepBytes, "step list too short");
+static_assert(2 * (2 * FieldGeom<0>::kSegMax + 1) <= kStepBytes, "step list too short");
+static_assert(FieldGeom<0>::kSegMax <= 32 && FieldGeom<1>::kSegMax <= 32, "one lane per staged row");
 constexpr uint32_t kTaskWords = (sizeof(MxkTask) + 3) / 4;
 static_assert(kTaskWords <= 32, "task descriptor must fit one warp's loads");
 static_assert(16 + kTaskWords * 4 <= kStepOffset, "header too small");
@@ -190,7 +192,7 @@ __device__ __forceinline__ void output_row(const uint8_t* buf, uint32_t c, uint1
     const uint32_t below = (1u << lane) - 1u;
     // step entries: (i * chunk bytes) | (u-flag << 4) | nibble; pass 0 (high
     // nibbles) is entries [0, n0), pass 1 (low nibbles) [n0, n_steps)
-    static_assert(G::kChunk == 2048 && G::kSeg <= 16, "step entries hold i * 2048 in 16 bits");
+    static_assert((G::kSegMax - 1) * G::kChunk + 31 < 65536, "step entries hold i * chunk | 31 in 16 bits");
     uint32_t n0 = 0, n_steps = 0;
 #pragma unroll
     for (int pass = 0; pass < 2; pass++) {
@@ -723,12 +725,11 @@ cudaError_t ensure_tables() {
     return e;
 }
 
-size_t smem_bytes(int gf16, int max_in) {
+// Shared memory of a launch staging seg_rows input rows per segment.
+size_t smem_bytes(int gf16, int seg_rows) {
     const int chunk = gf16 ? FieldGeom<1>::kChunk : FieldGeom<0>::kChunk;
-    const int segmax = gf16 ? FieldGeom<1>::kSeg : FieldGeom<0>::kSeg;
-    const int elem = gf16 ? 2 : 1;
-    const int seg = std::max(1, std::min(max_in, segmax));
-    (void)elem;
+    const int segmax = gf16 ? FieldGeom<1>::kSegMax : FieldGeom<0>::kSegMax;
+    const int seg = std::max(1, std::min(seg_rows, segmax));
     return (size_t)kSmemHeader + (size_t)seg * chunk;
 }
 
@@ -737,12 +738,14 @@ cudaError_t set_mxk_attrs() {
     using G = FieldGeom<kGf16>;
     static uint64_t done = 0;
     if (!first_on_device(done)) return cudaSuccess;
-    const int smem = (int)smem_bytes(kGf16, G::kSeg);
-    cudaError_t e = cudaFuncSetAttribute(mxk_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(mxk_single_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const int smem = (int)smem_bytes(kGf16, G::kSegMax);
+    cudaError_t e = cudaFuncSetAttribute(mxk_single_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(mxk_ksplit_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if constexpr (!kGf16) {  // the persistent drain serves GF(256) stripe batches
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(mxk_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    }
     if (e != cudaSuccess) done = 0;
     return e;
 }
@@ -794,46 +797,32 @@ cudaError_t launch_single_impl(const MxkTask& T, int32_t* status, int grid, cuda
     }
     const uint32_t items = T.n_items * (T.n_out ? (T.n_out + per - 1) / per : 1);
     if (grid <= 0 || grid > (int)items) grid = (int)items;
-    mxk_single_kernel<kGf16><<<grid, kThreads, smem_bytes(kGf16, T.n_in), stream>>>(T, status, seg_cap, per);
-    return cudaGetLastError();
-}
-
-template <int kGf16>
-cudaError_t launch_mxk_impl(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
-                            uint32_t* counter, int32_t* status, int max_in, int grid, cudaStream_t stream) {
-    using G = FieldGeom<kGf16>;
-    if (item_end <= item_lo) return cudaSuccess;
-    int seg_cap = std::max(1, std::min(max_in, G::kSeg));
-    cudaError_t e = set_mxk_attrs<kGf16>();
-    if (e != cudaSuccess) return e;
-    if (grid <= 0 || grid > (int)(item_end - item_lo)) grid = (int)(item_end - item_lo);
-    mxk_kernel<kGf16><<<grid, kThreads, smem_bytes(kGf16, max_in), stream>>>(tasks, item_task, item_lo, item_end,
-                                                                           counter, status, seg_cap);
+    mxk_single_kernel<kGf16><<<grid, kThreads, smem_bytes(kGf16, seg_cap), stream>>>(T, status, seg_cap, per);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-size_t mxk_smem_bytes(int gf16, int max_in) { return smem_bytes(gf16, max_in); }
+int mxk_default_seg(int max_in) { return std::max(1, std::min(max_in, FieldGeom<0>::kSeg)); }
 
-int mxk_ctas_per_sm(int gf16, int max_in) {
+int mxk_ctas_per_sm(int seg_rows) {
     int n = 0;
-    if ((gf16 ? set_mxk_attrs<1>() : set_mxk_attrs<0>()) != cudaSuccess) return 1;
-    const size_t smem = smem_bytes(gf16, max_in);
-    cudaError_t e = gf16 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mxk_kernel<1>, kThreads, smem)
-                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mxk_kernel<0>, kThreads, smem);
+    if (set_mxk_attrs<0>() != cudaSuccess) return 1;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mxk_kernel<0>, kThreads, smem_bytes(0, seg_rows));
     if (e != cudaSuccess || n < 1) n = 1;
     return n;
 }
 
 cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
-                             uint32_t* counter, int32_t* status, int max_in, int grid, cudaStream_t stream) {
-    return launch_mxk_impl<0>(tasks, item_task, item_lo, item_end, counter, status, max_in, grid, stream);
-}
-
-cudaError_t launch_gf16_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
-                            uint32_t* counter, int32_t* status, int max_in, int grid, cudaStream_t stream) {
-    return launch_mxk_impl<1>(tasks, item_task, item_lo, item_end, counter, status, max_in, grid, stream);
+                             uint32_t* counter, int32_t* status, int seg_rows, int grid, cudaStream_t stream) {
+    if (item_end <= item_lo) return cudaSuccess;
+    if (seg_rows < 1 || seg_rows > FieldGeom<0>::kSegMax) return cudaErrorInvalidValue;
+    cudaError_t e = set_mxk_attrs<0>();
+    if (e != cudaSuccess) return e;
+    if (grid <= 0 || grid > (int)(item_end - item_lo)) grid = (int)(item_end - item_lo);
+    mxk_kernel<0><<<grid, kThreads, smem_bytes(0, seg_rows), stream>>>(tasks, item_task, item_lo, item_end, counter,
+                                                                       status, seg_rows);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream) {

@@ -9,6 +9,8 @@ import time
 from dataclasses import dataclass
 from typing import List, Optional, Sequence
 
+import numpy as np
+
 from .api import Library, _Error, make_error
 
 OP_ENCODE = 0
@@ -91,8 +93,10 @@ class Server:
                indices: Optional[Sequence[int]] = None, tag: int = 0) -> int:
         r = _Request(op, int(engine), k, m, symbol_len, in_ptr, out_ptr, None, tag)
         if indices is not None:
-            arr = (C.c_uint64 * len(indices))(*[int(i) for i in indices])
-            r.indices = C.cast(arr, C.POINTER(C.c_uint64))
+            # one conversion for the whole list (a uint64 array passes through
+            # as is); the server copies the indices before returning
+            arr = np.ascontiguousarray(indices, dtype=np.uint64)
+            r.indices = arr.ctypes.data_as(C.POINTER(C.c_uint64))
         t = C.c_uint64()
         err = _Error()
         self._lib.check(self._lib.lib.scrs_server_submit(self._ptr, C.byref(r), C.byref(t), C.byref(err)), err)

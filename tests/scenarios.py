@@ -92,3 +92,54 @@ def direct_gf256_repairs(engine_coeffs, data, k, m, L):
         for i in range(k):
             out[j] ^= gfpy.scale_bytes(rows[i], engine_coeffs[i * m + j])
     return out.reshape(-1)
+
+
+def device_stripes(torch, oracle, specs, rng):
+    """Device buffers for (op, engine, k, m, L) specs: encode stripes of random
+    data, decode stripes of k received rows (random erasures, shuffled order).
+    Returns (stripes, output tensors, expected bytes, tensors to keep alive)."""
+    from scrs_b200.batch import OP_ENCODE, Stripe
+
+    stripes, expect, outs, keep = [], [], [], []
+    for op, engine, k, m, L in specs:
+        p = oracle.resolve(engine, k, m, L)
+        data = rng.integers(0, 256, k * L, dtype=np.uint8)
+        if op == OP_ENCODE:
+            exp = np.zeros(m * L, np.uint8)
+            oracle.batch_encoder(p).encode_into(data, exp)
+            d_in = torch.from_numpy(data).cuda()
+            d_out = torch.zeros(m * L, dtype=torch.uint8, device="cuda")
+            stripes.append(Stripe(op, engine, k, m, L, d_in.data_ptr(), d_out.data_ptr()))
+            expect.append(exp)
+        else:
+            word = encode_word(oracle, p, data)
+            e = int(rng.integers(0, min(k, m) + 1))
+            erased = rng.choice(k, e, replace=False).tolist()
+            repairs = rng.choice(m, e, replace=False).tolist()
+            idx = [i for i in range(k) if i not in erased] + [k + j for j in repairs]
+            idx = rng.permutation(idx).tolist()
+            d_in = torch.from_numpy(np.concatenate([word[i] for i in idx])).cuda()
+            d_out = torch.zeros(k * L, dtype=torch.uint8, device="cuda")
+            stripes.append(Stripe(op, engine, k, m, L, d_in.data_ptr(), d_out.data_ptr(), idx))
+            expect.append(data)
+        keep.append(d_in)
+        outs.append(d_out)
+    return stripes, outs, expect, keep
+
+
+def make_mixed_batch(torch, n_stripes, seed, lens=(1024, 4096, 65536), kmax=64, mmax=16):
+    """(op, engine, k, m, L) specs of a mixed GF(256) stripe batch: k ~ U[4, kmax],
+    m ~ U[1, mmax], L from `lens`, Standard or Good Cauchy, encode and decode
+    alternating.  Returns (specs, the generator for the stripes' contents)."""
+    from scrs_b200.batch import OP_DECODE, OP_ENCODE
+
+    rng = np.random.default_rng(seed)
+    specs = []
+    for s in range(n_stripes):
+        k = int(rng.integers(4, kmax + 1))
+        m = int(rng.integers(1, mmax + 1))
+        L = int(rng.choice(lens))
+        engine = Engine.STANDARD_CAUCHY if rng.integers(0, 2) else Engine.GOOD_CAUCHY
+        op = OP_ENCODE if s % 2 == 0 else OP_DECODE
+        specs.append((op, engine, k, m, L))
+    return specs, rng

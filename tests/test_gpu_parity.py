@@ -7,8 +7,8 @@ import pytest
 from scrs_b200.api import DEPENDENT, DecodeError, EncodeError, Engine, PushOutcome
 
 import gfpy
-from scenarios import (batch_decode, deterministic_subsets, encode_word, k_subsets, lazy_decode,
-                       lcg_permutations)
+from scenarios import (batch_decode, deterministic_subsets, device_stripes, encode_word, k_subsets, lazy_decode,
+                       lcg_permutations, make_mixed_batch)
 
 pytestmark = pytest.mark.gpu
 
@@ -272,50 +272,12 @@ def test_device_pointer_entry_points(gpu, oracle):
 
 # ---------------------------------------------------------------- batched stripes
 
-def make_mixed_batch(torch, n_stripes, seed, lens=(1024, 4096, 65536), kmax=64, mmax=16):
-    from scrs_b200.batch import OP_DECODE, OP_ENCODE, Stripe
-
-    rng = np.random.default_rng(seed)
-    specs = []
-    for s in range(n_stripes):
-        k = int(rng.integers(4, kmax + 1))
-        m = int(rng.integers(1, mmax + 1))
-        L = int(rng.choice(lens))
-        engine = Engine.STANDARD_CAUCHY if rng.integers(0, 2) else Engine.GOOD_CAUCHY
-        op = OP_ENCODE if s % 2 == 0 else OP_DECODE
-        specs.append((op, engine, k, m, L))
-    return specs, rng
-
-
 def test_stripe_batch_matches_oracle(gpu, oracle):
     torch = pytest.importorskip("torch")
-    from scrs_b200.batch import OP_DECODE, OP_ENCODE, Stripe, StripeBatch
+    from scrs_b200.batch import StripeBatch
 
     specs, rng = make_mixed_batch(torch, 96, 4, lens=(1024, 4096, 1000, 64))
-    stripes, expect, outs, keep = [], [], [], []
-    for op, engine, k, m, L in specs:
-        p = oracle.resolve(engine, k, m, L)
-        data = rng.integers(0, 256, k * L, dtype=np.uint8)
-        if op == OP_ENCODE:
-            exp = np.zeros(m * L, np.uint8)
-            oracle.batch_encoder(p).encode_into(data, exp)
-            d_in = torch.from_numpy(data).cuda()
-            d_out = torch.zeros(m * L, dtype=torch.uint8, device="cuda")
-            stripes.append(Stripe(op, engine, k, m, L, d_in.data_ptr(), d_out.data_ptr()))
-            expect.append(exp)
-        else:
-            word = encode_word(oracle, p, data)
-            e = int(rng.integers(0, min(k, m) + 1))
-            erased = rng.choice(k, e, replace=False).tolist()
-            repairs = rng.choice(m, e, replace=False).tolist()
-            idx = [i for i in range(k) if i not in erased] + [k + j for j in repairs]
-            idx = rng.permutation(idx).tolist()
-            d_in = torch.from_numpy(np.concatenate([word[i] for i in idx])).cuda()
-            d_out = torch.zeros(k * L, dtype=torch.uint8, device="cuda")
-            stripes.append(Stripe(op, engine, k, m, L, d_in.data_ptr(), d_out.data_ptr(), idx))
-            expect.append(data)
-        keep.append(d_in)
-        outs.append(d_out)
+    stripes, outs, expect, keep = device_stripes(torch, oracle, specs, rng)
     b = StripeBatch(gpu.lib, len(stripes))
     b.set(stripes)
     for mode in ("persistent", "graph", "plain", "graph"):
