@@ -385,26 +385,32 @@ cudaError_t run_transform(uint8_t* work, uint32_t G, int D, const uint16_t* fact
             return e;
         }
     }
-    const uint32_t gt = std::min<uint32_t>(G, 16);
+    // Column groups per tile: up to 8 of one row pair, so that the lanes of a
+    // warp (consecutive groups of a few pairs) mostly share the butterfly
+    // factor, and tiles stay small enough for two-level-count passes
+    // (k = m = 4096, L = 1024: 8 groups give 2 passes of 6-7 levels, 16 gave 3).
+    const uint32_t gt = std::min<uint32_t>(G, 8);
     int cmax = 1;
     while (cmax < D && ((size_t)2 << cmax) * gt * 64 <= (size_t)kTileBytes) cmax++;
-    // the fewest passes the tile size allows, with levels spread evenly over
-    // them: smaller tiles for the same traffic, so more CTAs per pass
+    const uint32_t col_tiles = (G + gt - 1) / gt;
+    // The fewest passes the tile size allows (a pass more costs more than the
+    // parallelism it adds), levels spread evenly over them.
     const int n_pass = (D + cmax - 1) / cmax;
-    const int cbal = (D + n_pass - 1) / n_pass;
     std::vector<std::pair<int, int>> passes;  // (l0, c) top-down
-    for (int l0 = 0; l0 < D;) {
-        int c = std::min(cbal, D - l0);
+    for (int q = 0, l0 = 0; q < n_pass; q++) {
+        const int c = D / n_pass + (q < D % n_pass ? 1 : 0);
         passes.push_back({l0, c});
         l0 += c;
     }
     if (!forward) std::reverse(passes.begin(), passes.end());
-    const uint32_t col_tiles = (G + gt - 1) / gt;
     for (auto& pc : passes) {
         const int l0 = pc.first, c = pc.second;
         const uint32_t tiles = (1u << (D - c)) * col_tiles;
         const size_t smem = ((size_t)1 << c) * gt * 64;
-        afft_pass_kernel<<<tiles, kPassThreads, smem, st>>>(work, G, D, 1, l0, c, forward ? 1 : 0, factors, gt);
+        // one butterfly per thread and level (a multiple of 32, at most kPassThreads)
+        const uint32_t bfly = (1u << (c - 1)) * gt;
+        const int threads = (int)std::min<uint32_t>(kPassThreads, std::max<uint32_t>(32, (bfly + 31) / 32 * 32));
+        afft_pass_kernel<<<tiles, threads, smem, st>>>(work, G, D, 1, l0, c, forward ? 1 : 0, factors, gt);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
