@@ -85,7 +85,8 @@ enum {
     SCRS_ERR_NO_DEVICE = 904,
     SCRS_ERR_CAPACITY = 905,      /* a = requested, b = limit              */
     SCRS_ERR_DEVICE_TIMEOUT = 906,/* a bounded device-side wait expired    */
-    SCRS_ERR_BAD_ARGUMENT = 907   /* a = argument position                 */
+    SCRS_ERR_BAD_ARGUMENT = 907,  /* a = argument position                 */
+    SCRS_ERR_JIT = 908            /* a = nvrtcResult of a failed run-time compile */
 };
 
 /* PushOutcome (symbol_sink.rs:11-26) */
@@ -371,6 +372,12 @@ SCRS_API uint64_t scrs_stripe_batch_last_launches(const scrs_stripe_batch* batch
 SCRS_API int32_t scrs_stripe_batch_run_timed(scrs_stripe_batch* batch, void* stream,
                                              float* plan_ms, float* drain_ms,
                                              scrs_error* err);
+/* As scrs_stripe_batch_run_timed, with the drain split: the kernels
+ * specialised to encode matrices (spec_ms, 0 when there are none) and the
+ * generic drain (generic_ms); drain_ms above is their sum. */
+SCRS_API int32_t scrs_stripe_batch_run_timed_drains(scrs_stripe_batch* batch, void* stream,
+                                                    float* plan_ms, float* spec_ms,
+                                                    float* generic_ms, scrs_error* err);
 /* After the run's stream has synchronised: SCRS_OK, or the device-side
  * failure a kernel recorded (SCRS_ERR_DEVICE_TIMEOUT). */
 SCRS_API int32_t scrs_stripe_batch_check(scrs_stripe_batch* batch, scrs_error* err);
@@ -421,6 +428,25 @@ SCRS_API int32_t scrs_stripe_batch_launch_params(const scrs_stripe_batch* batch,
  * inputs.  Synchronises `stream`. */
 SCRS_API int32_t scrs_stripe_batch_autotune(scrs_stripe_batch* batch, void* stream, uint32_t reps,
                                             scrs_tune_params* chosen, scrs_error* err);
+/* ---- Encode kernels specialised to one coefficient matrix ------------------
+ * No reference counterpart.  Encode stripes of a GF(256) engine with
+ * k <= 32 and k*m <= 64 run, inside stripe batches, through a drain kernel
+ * generated for their (engine, k, m) matrix (every coefficient's XOR network
+ * inlined) and compiled for sm_100a by NVRTC on first use; the kernel is
+ * cached for the life of the process.  scrs_jit_prepare compiles (and, with
+ * load != 0, loads for the current device) ahead of time, so the first
+ * batch does not pay the compile; without load it needs no device.
+ * SCRS_ERR_BAD_ARGUMENT for an engine or geometry that is not specialised,
+ * SCRS_ERR_JIT (a = nvrtcResult) when the compile fails. */
+SCRS_API int32_t scrs_jit_prepare(int32_t engine, uint32_t k, uint32_t m, int32_t load,
+                                  uint64_t* cubin_bytes, scrs_error* err);
+/* Whether scrs_stripe_batch_set specialises eligible encode stripes (1, the
+ * default) or runs every stripe through the generic drain (0).  Takes
+ * effect at the next set. */
+SCRS_API int32_t scrs_stripe_batch_set_jit(scrs_stripe_batch* batch, int32_t enable, scrs_error* err);
+/* Stripes of the current descriptors that run through specialised kernels. */
+SCRS_API uint64_t scrs_stripe_batch_jit_stripes(const scrs_stripe_batch* batch);
+
 /* The table (for saving and loading it): entries 0..size-1, set, clear. */
 SCRS_API uint64_t scrs_tune_table_size(void);
 SCRS_API int32_t scrs_tune_table_entry(uint64_t i, scrs_tune_key* key, scrs_tune_params* params,

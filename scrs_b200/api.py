@@ -89,6 +89,7 @@ _STATUS = {
     905: ("RuntimeFailure", "Capacity", ("requested", "limit")),
     906: ("RuntimeFailure", "DeviceTimeout", ()),
     907: ("RuntimeFailure", "BadArgument", ("position",)),
+    908: ("RuntimeFailure", "Jit", ("nvrtc_result",)),
 }
 
 

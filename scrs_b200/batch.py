@@ -70,7 +70,26 @@ def _bind(lib: Library):
                                               C.POINTER(_Error)]
     L.scrs_stripe_batch_check.restype = C.c_int32
     L.scrs_stripe_batch_check.argtypes = [C.c_void_p, C.POINTER(_Error)]
+    L.scrs_stripe_batch_run_timed_drains.restype = C.c_int32
+    L.scrs_stripe_batch_run_timed_drains.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_float),
+                                                     C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(_Error)]
+    L.scrs_stripe_batch_set_jit.restype = C.c_int32
+    L.scrs_stripe_batch_set_jit.argtypes = [C.c_void_p, C.c_int32, C.POINTER(_Error)]
+    L.scrs_stripe_batch_jit_stripes.restype = C.c_uint64
+    L.scrs_stripe_batch_jit_stripes.argtypes = [C.c_void_p]
+    L.scrs_jit_prepare.restype = C.c_int32
+    L.scrs_jit_prepare.argtypes = [C.c_int32, C.c_uint32, C.c_uint32, C.c_int32, C.POINTER(C.c_uint64),
+                                   C.POINTER(_Error)]
     lib._batch_bound = True
+
+
+def jit_prepare(lib: Library, engine, k: int, m: int, load: bool = True) -> int:
+    """Compile (and with ``load`` load) the encode kernel specialised to the
+    (engine, k, m) matrix ahead of its first batch; returns its cubin size."""
+    _bind(lib)
+    n, err = C.c_uint64(), _Error()
+    lib.check(lib.lib.scrs_jit_prepare(int(engine), k, m, 1 if load else 0, C.byref(n), C.byref(err)), err)
+    return n.value
 
 
 class StripeBatch:
@@ -136,6 +155,23 @@ class StripeBatch:
         self._lib.check(self._lib.lib.scrs_stripe_batch_run_timed(self._ptr, _stream_ptr(stream), C.byref(a),
                                                                   C.byref(b), C.byref(err)), err)
         return a.value, b.value
+
+    def run_timed_drains(self, stream=None):
+        """(plan_ms, specialised_drains_ms, generic_drain_ms) of one non-graph run."""
+        err, a, b, c = _Error(), C.c_float(), C.c_float(), C.c_float()
+        self._lib.check(self._lib.lib.scrs_stripe_batch_run_timed_drains(self._ptr, _stream_ptr(stream), C.byref(a),
+                                                                         C.byref(b), C.byref(c), C.byref(err)), err)
+        return a.value, b.value, c.value
+
+    def set_jit(self, enable: bool):
+        """Specialise eligible encode stripes at the next set (default on)."""
+        err = _Error()
+        self._lib.check(self._lib.lib.scrs_stripe_batch_set_jit(self._ptr, 1 if enable else 0, C.byref(err)), err)
+
+    @property
+    def jit_stripes(self) -> int:
+        """Stripes of the current descriptors that run through specialised kernels."""
+        return int(self._lib.lib.scrs_stripe_batch_jit_stripes(self._ptr))
 
     def run_plain(self, stream=None):
         err = _Error()

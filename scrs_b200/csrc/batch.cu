@@ -22,6 +22,7 @@
 #include <tuple>
 
 #include "host_field.h"
+#include "jit.h"
 #include "runtime.h"
 #include "tune.h"
 
@@ -37,6 +38,17 @@ struct scrs_stripe_batch {
     std::vector<uint8_t> arena;
     uint32_t total_items = 0, max_in = 1, max_plan_r = 0;
     scrs_tune_key key{};  // geometry key of the current descriptors (autotuner table)
+    // Encode groups of one (engine, k, m) run through a kernel specialised to
+    // their matrix (jit.cu): items [item_lo, item_hi) each; the generic drain
+    // takes items [gen_lo, total_items).
+    struct SpecRun {
+        JitKernel jk;
+        uint32_t item_lo, item_hi;
+        uint64_t stripes;
+    };
+    bool jit = true;
+    std::vector<SpecRun> spec;
+    uint32_t gen_lo = 0;
     cudaGraphExec_t graph = nullptr;
     uint64_t graph_version = 0;   // autotuner table version the graph was captured under
     uint64_t graph_launches = 0;  // kernels in the captured graph
@@ -73,6 +85,9 @@ struct scrs_stripe_batch {
 
 namespace {
 constexpr size_t kMaxPieces = 16;  // one work counter each in d_counter
+constexpr size_t kMaxSpecRuns = 4;  // specialised groups per batch (counters 1..4)
+// A group is specialised when it has at least one persistent grid of items.
+constexpr uint64_t kJitMinItems = 8 * 148;
 }
 
 extern "C" int32_t scrs_stripe_batch_create(uint64_t max_stripes, uint64_t max_items, scrs_stripe_batch** out,
@@ -247,6 +262,52 @@ int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc
     b->total_items = item;
     b->max_in = max_in;
     b->key = tune_key_of(descs, count);
+    // ---- encode groups with a specialised kernel take the first item ranges
+    b->spec.clear();
+    b->gen_lo = 0;
+    if (b->jit) {
+        std::map<std::tuple<int, uint32_t, uint32_t>, std::vector<uint32_t>> groups;
+        std::vector<std::tuple<int, uint32_t, uint32_t>> order;  // first appearance
+        for (uint64_t s = 0; s < count; s++) {
+            const scrs_stripe_desc& d = descs[s];
+            if (d.op != SCRS_OP_ENCODE || !jit_eligible(d.k, d.m)) continue;
+            auto key = std::make_tuple(d.engine, d.k, d.m);
+            auto& g = groups[key];
+            if (g.empty()) order.push_back(key);
+            g.push_back((uint32_t)s);
+        }
+        std::vector<char> in_spec(count, 0);
+        uint32_t next = 0;
+        for (auto& key : order) {
+            if (b->spec.size() == kMaxSpecRuns) break;
+            auto& g = groups[key];
+            uint64_t n = 0;
+            for (uint32_t t : g) n += b->tasks[t].n_items;
+            JitKernel jk{};
+            scrs_error je{};
+            if (n < kJitMinItems ||
+                jit_kernel(std::get<0>(key), std::get<1>(key), std::get<2>(key), true, &jk, &je) != SCRS_OK)
+                continue;  // too small to fill the GPU, or not compiled: the generic drain runs it
+            const uint32_t lo = next;
+            for (uint32_t t : g) {
+                b->tasks[t].item_begin = next;
+                next += b->tasks[t].n_items;
+                in_spec[t] = 1;
+            }
+            b->spec.push_back({jk, lo, next, (uint64_t)g.size()});
+        }
+        if (!b->spec.empty()) {
+            b->gen_lo = next;
+            uint32_t gen_max_in = 1;
+            for (uint64_t t = 0; t < count; t++) {
+                if (in_spec[t]) continue;
+                b->tasks[t].item_begin = next;
+                next += b->tasks[t].n_items;
+                gen_max_in = std::max(gen_max_in, b->tasks[t].n_in);
+            }
+            b->max_in = gen_max_in;
+        }
+    }
     b->item_task.resize(item);
     for (size_t t = 0; t < b->tasks.size(); t++)
         std::fill(b->item_task.begin() + b->tasks[t].item_begin,
@@ -354,7 +415,10 @@ extern "C" int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* b, const scrs_s
         oo += (ob + 15) & ~(size_t)15;
         if (s + 1 == cut[piece + 1]) piece++;
     }
+    const bool jit = b->jit;  // pieces are stripe ranges: keep the items in stripe order
+    b->jit = false;
     int32_t r = scrs_stripe_batch_set(b, dev.data(), count, err);
+    b->jit = jit;
     if (r) return r;
     b->pieces.clear();
     for (size_t q = 0; q + 1 < cut.size(); q++) {
@@ -434,24 +498,39 @@ DrainCfg drain_cfg(const scrs_stripe_batch* b) {
     }
     const int fit = mxk_ctas_per_sm(c.seg_rows);
     if (c.ctas_per_sm <= 0 || c.ctas_per_sm > fit) c.ctas_per_sm = fit;
-    c.grid = std::max(1, std::min<int>(b->sm_count * c.ctas_per_sm, (int)std::max<uint32_t>(b->total_items, 1)));
+    const uint32_t items = b->total_items - b->gen_lo;
+    c.grid = std::max(1, std::min<int>(b->sm_count * c.ctas_per_sm, (int)std::max<uint32_t>(items, 1)));
     return c;
 }
 
+// The drains of a device-resident run: the specialised groups' kernels, then
+// the generic drain (work counter q + 1 for group q, 0 for the generic one).
+int32_t enqueue_drains(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err, bool run_spec = true,
+                       bool run_generic = true) {
+    for (size_t q = 0; run_spec && q < b->spec.size(); q++) {
+        const scrs_stripe_batch::SpecRun& R = b->spec[q];
+        SCRS_CUDA(launch_jit(R.jk, b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), R.item_lo, R.item_hi,
+                             b->d_counter.as<uint32_t>() + 1 + q, b->status.dev, b->sm_count * R.jk.ctas_per_sm, st));
+        b->last_launches++;
+    }
+    if (run_generic && b->total_items > b->gen_lo) {
+        const DrainCfg c = drain_cfg(b);
+        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), b->gen_lo,
+                                   b->total_items, b->d_counter.as<uint32_t>(), b->status.dev, c.seg_rows, c.grid,
+                                   st));
+        b->last_launches++;
+    }
+    return SCRS_OK;
+}
+
 int32_t enqueue_batch(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
-    SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, 4, st));
+    SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, (1 + b->spec.size()) * sizeof(uint32_t), st));
     b->last_launches = 0;
     if (!b->plans.empty()) {
         SCRS_CUDA(launch_cauchy_plan(b->d_plans.as<CauchyPlanTask>(), (uint32_t)b->plans.size(), 0, b->max_plan_r, st));
         b->last_launches++;
     }
-    if (b->total_items) {
-        const DrainCfg c = drain_cfg(b);
-        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), 0, b->total_items,
-                                   b->d_counter.as<uint32_t>(), b->status.dev, c.seg_rows, c.grid, st));
-        b->last_launches++;
-    }
-    return SCRS_OK;
+    return enqueue_drains(b, st, err);
 }
 
 // Host-buffer run: copies and compute of consecutive pieces overlap (see top).
@@ -565,11 +644,19 @@ extern "C" int32_t scrs_stripe_batch_run_plain(scrs_stripe_batch* b, void* strea
 
 extern "C" int32_t scrs_stripe_batch_run_timed(scrs_stripe_batch* b, void* stream, float* plan_ms,
                                                float* drain_ms, scrs_error* err) {
+    float spec = 0, gen = 0;
+    int32_t rc = scrs_stripe_batch_run_timed_drains(b, stream, plan_ms, &spec, &gen, err);
+    if (!rc && drain_ms) *drain_ms = spec + gen;
+    return rc;
+}
+
+extern "C" int32_t scrs_stripe_batch_run_timed_drains(scrs_stripe_batch* b, void* stream, float* plan_ms,
+                                                      float* spec_ms, float* generic_ms, scrs_error* err) {
     if (!b) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
     cudaStream_t st = (cudaStream_t)stream;
-    cudaEvent_t ev[3];
+    cudaEvent_t ev[4];
     for (auto& e : ev) SCRS_CUDA(cudaEventCreate(&e));
-    SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, 4, st));
+    SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, (1 + b->spec.size()) * sizeof(uint32_t), st));
     b->last_launches = 0;
     cudaEventRecord(ev[0], st);
     if (!b->plans.empty()) {
@@ -577,20 +664,19 @@ extern "C" int32_t scrs_stripe_batch_run_timed(scrs_stripe_batch* b, void* strea
         b->last_launches++;
     }
     cudaEventRecord(ev[1], st);
-    if (b->total_items) {
-        const DrainCfg c = drain_cfg(b);
-        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), 0, b->total_items,
-                                   b->d_counter.as<uint32_t>(), b->status.dev, c.seg_rows, c.grid, st));
-        b->last_launches++;
-    }
+    int32_t rc = enqueue_drains(b, st, err, false, true);
+    if (rc) return rc;
     cudaEventRecord(ev[2], st);
-    SCRS_CUDA(cudaEventSynchronize(ev[2]));
-    float a = 0, c = 0;
-    cudaEventElapsedTime(&a, ev[0], ev[1]);
-    cudaEventElapsedTime(&c, ev[1], ev[2]);
+    rc = enqueue_drains(b, st, err, true, false);
+    if (rc) return rc;
+    cudaEventRecord(ev[3], st);
+    SCRS_CUDA(cudaEventSynchronize(ev[3]));
+    float t[3] = {0, 0, 0};
+    for (int i = 0; i < 3; i++) cudaEventElapsedTime(&t[i], ev[i], ev[i + 1]);
     for (auto& e : ev) cudaEventDestroy(e);
-    if (plan_ms) *plan_ms = a;
-    if (drain_ms) *drain_ms = c;
+    if (plan_ms) *plan_ms = t[0];
+    if (generic_ms) *generic_ms = t[1];
+    if (spec_ms) *spec_ms = t[2];
     return set_err(err, SCRS_OK);
 }
 
@@ -624,8 +710,8 @@ int32_t time_drain(scrs_stripe_batch* b, cudaStream_t st, int seg_rows, int grid
     for (uint32_t rep = 0; rep <= reps; rep++) {
         SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, 4, st));
         SCRS_CUDA(cudaEventRecord(e0, st));
-        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), 0, b->total_items,
-                                   b->d_counter.as<uint32_t>(), b->status.dev, seg_rows, grid, st));
+        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), b->gen_lo,
+                                   b->total_items, b->d_counter.as<uint32_t>(), b->status.dev, seg_rows, grid, st));
         SCRS_CUDA(cudaEventRecord(e1, st));
         SCRS_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
@@ -645,7 +731,7 @@ extern "C" int32_t scrs_stripe_batch_autotune(scrs_stripe_batch* b, void* stream
     if (reps > 100) return set_err(err, SCRS_ERR_BAD_ARGUMENT, 3, reps);
     if (reps == 0) reps = 5;
     cudaStream_t st = (cudaStream_t)stream;
-    if (b->total_items == 0) return scrs_stripe_batch_launch_params(b, chosen, err);
+    if (b->total_items <= b->gen_lo) return scrs_stripe_batch_launch_params(b, chosen, err);
     // inputs on the device and decode matrices built before any drain
     if (b->host_mode) {
         int32_t r = run_host(b, st, err);
@@ -673,7 +759,7 @@ extern "C" int32_t scrs_stripe_batch_autotune(scrs_stripe_batch* b, void* stream
             if (std::find(ctas.begin(), ctas.end(), c) == ctas.end()) ctas.push_back(c);
         }
         for (int c : ctas) {
-            const int grid = std::max(1, std::min<int>(b->sm_count * c, (int)b->total_items));
+            const int grid = std::max(1, std::min<int>(b->sm_count * c, (int)(b->total_items - b->gen_lo)));
             float ms = 0;
             rc = time_drain(b, st, seg, grid, reps, e0, e1, &ms, err);
             if (rc) break;
@@ -695,4 +781,17 @@ extern "C" int32_t scrs_stripe_batch_autotune(scrs_stripe_batch* b, void* stream
     }
     *chosen = best;
     return set_err(err, SCRS_OK);
+}
+
+extern "C" int32_t scrs_stripe_batch_set_jit(scrs_stripe_batch* b, int32_t enable, scrs_error* err) {
+    if (!b) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
+    b->jit = enable != 0;
+    return set_err(err, SCRS_OK);
+}
+
+extern "C" uint64_t scrs_stripe_batch_jit_stripes(const scrs_stripe_batch* b) {
+    uint64_t n = 0;
+    if (b)
+        for (auto& R : b->spec) n += R.stripes;
+    return n;
 }

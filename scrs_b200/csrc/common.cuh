@@ -1,10 +1,12 @@
 // Shared device/host helpers for the sm_100a erasure-coding kernels.
 #pragma once
 
+#ifndef __CUDACC_RTC__  // the run-time compiler (jit.cu) supplies stdint.h and the status codes
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "../../include/scrs_gpu.h"
+#endif
 
 #define SCRS_HD __host__ __device__ __forceinline__
 
@@ -12,7 +14,7 @@ namespace scrs {
 
 // ---- GF(256): polynomial 0x11B, generator 3 (scrs/src/algebra/gf256.rs) ----
 // Compile-time product used to build the per-coefficient XOR networks.
-constexpr uint8_t gf8_mul_ce(uint8_t a, uint8_t b) {
+__host__ __device__ constexpr uint8_t gf8_mul_ce(uint8_t a, uint8_t b) {
     uint8_t acc = 0;
     for (int i = 0; i < 8; i++) {
         if ((b >> i) & 1) acc ^= a;
@@ -24,7 +26,7 @@ constexpr uint8_t gf8_mul_ce(uint8_t a, uint8_t b) {
 }
 
 // Bit r of (c * x^s): entry (r, s) of the 8x8 GF(2) matrix of "multiply by c".
-constexpr bool gf8_matrix_bit(int c, int r, int s) {
+__host__ __device__ constexpr bool gf8_matrix_bit(int c, int r, int s) {
     return (gf8_mul_ce((uint8_t)c, (uint8_t)(1u << s)) >> r) & 1;
 }
 

@@ -237,6 +237,7 @@ extern "C" const char* scrs_status_name(int32_t code) {
         case SCRS_ERR_CAPACITY: return "Capacity";
         case SCRS_ERR_DEVICE_TIMEOUT: return "DeviceTimeout";
         case SCRS_ERR_BAD_ARGUMENT: return "BadArgument";
+        case SCRS_ERR_JIT: return "Jit";
         default: return "Unknown";
     }
 }

@@ -2,11 +2,14 @@
 // the host engine code.
 #pragma once
 
+#ifndef __CUDACC_RTC__  // the run-time compiler (jit.cu) sees only the device parts
 #include <cuda_runtime.h>
 #include <stdint.h>
+#endif
 
 namespace scrs {
 
+#ifndef __CUDACC_RTC__
 // Per-device one-time set-up flags (function attributes such as the dynamic
 // shared-memory limit are set per device): true the first time it is called
 // for the current device, false afterwards.
@@ -18,6 +21,7 @@ inline bool first_on_device(uint64_t& done_mask) {
     done_mask |= bit;
     return true;
 }
+#endif
 
 constexpr uint16_t kNoRow = 0xFFFFu;
 constexpr int kThreads = 128;   // 4 warps per CTA
@@ -77,6 +81,7 @@ struct CauchyPlanTask {
     uint32_t* work;           // 4*r words of global scratch, or nullptr (shared memory)
 };
 
+#ifndef __CUDACC_RTC__
 // Launchers (return cudaError_t of the launch).
 // Persistent drain of the work items [item_lo, item_end): item i belongs to
 // tasks[item_task[i]] (row chunk i - item_begin of that task).  work_counter
@@ -106,5 +111,6 @@ int mxk_default_seg(int max_in);
 // Most CTAs of the GF(256) persistent drain one SM holds with seg_rows rows
 // staged per segment (shared memory and registers permitting).
 int mxk_ctas_per_sm(int seg_rows);
+#endif  // __CUDACC_RTC__
 
 }  // namespace scrs

@@ -229,6 +229,7 @@ int32_t launch_single(scrs_server* s, Slot& sl, Req& r, scrs_error* err) {
 int32_t launch_group(Slot& sl, std::vector<Req>& group, scrs_error* err) {
     if (!sl.batch) {
         int32_t rc = scrs_stripe_batch_create(kMaxCoalesce, 0, &sl.batch, err);
+        if (!rc) rc = scrs_stripe_batch_set_jit(sl.batch, 0, err);  // no compile inside a request's latency
         if (rc) return rc;
     }
     std::vector<scrs_stripe_desc> d(group.size());
