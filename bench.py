@@ -405,11 +405,15 @@ def extra_latency(torch, api):
     return res
 
 
+RATES_PER_S = (2500.0, 5000.0, 10000.0)  # offered Poisson arrival rates of the serving sweep
+
+
 def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C250005):
     """Config 5: Poisson arrivals of mixed encode/decode requests over all four
     engines through the serving loop (scrs_server_*), 64 GB budget, 8 slots.
-    The rate sweep is 0.25x, 0.5x and 0.75x the closed-loop capacity measured
-    first (median of three passes).  Payloads are seeded random device bytes (decode requests decode
+    The closed-loop capacity (2000 requests submitted at once, median of three
+    passes) is reported beside a sweep of fixed Poisson rates, so that runs on
+    different hosts compare at the same offered load.  Payloads are seeded random device bytes (decode requests decode
     random received rows: the same work; bit-exactness is covered by the
     serving tests).  Latency = completion seen by the host - submit."""
     from scrs_b200.api import Engine
@@ -470,8 +474,7 @@ def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C25
            "closed_loop": {"requests_per_s": round(cap_rate, 1), "goodput_GBps": round(cap_gbps / 1e9, 2),
                            "passes_requests_per_s": [round(r, 1) for r, _ in passes]},
            "rates": []}
-    for frac in (0.25, 0.5, 0.75):
-        rate = frac * cap_rate
+    for rate in RATES_PER_S:
         n = int(rate * seconds_per_rate)
         arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
         picks = rng.integers(0, len(templates), n)
