@@ -10,6 +10,7 @@
 #include <map>
 #include <mutex>
 #include <new>
+#include <type_traits>
 
 #include "afft_engine.h"
 #include "gf_mul_core.cuh"
@@ -280,14 +281,21 @@ __global__ void __launch_bounds__(128) scale_out_kernel(const uint8_t* work, uin
     }
 }
 
+// dst row rows[t] = src row (row_map ? row_map[rows[t]] : rows[t]), L bytes
+// each, in units of `unit` bytes (16 when both bases are 16-byte aligned and
+// L is a multiple of 16, else 1).
+template <int kUnit>
 __global__ void copy_rows_kernel(const uint8_t* src, uint8_t* dst, uint64_t L, const uint16_t* rows,
                                  uint32_t count, const uint16_t* row_map) {
-    const uint64_t total = (uint64_t)count * L;
+    using U = typename std::conditional<kUnit == 16, uint4, uint8_t>::type;
+    const uint64_t per = L / kUnit;
+    const uint64_t total = (uint64_t)count * per;
     for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < total;
          x += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t r = rows[x / L];
+        const uint64_t t = x / per, q = x - t * per;
+        const uint64_t r = rows[t];
         const uint64_t s = row_map ? row_map[r] : r;
-        dst[r * L + x % L] = src[s * L + x % L];
+        reinterpret_cast<U*>(dst + r * L)[q] = reinterpret_cast<const U*>(src + s * L)[q];
     }
 }
 
@@ -694,7 +702,14 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
         d_map = ws.row_map.as<uint16_t>();
     }
     if (np) {
-        copy_rows_kernel<<<grid_for((uint64_t)np * L, 256), 256, 0, st>>>(d_payloads, d_out, L, d_pres, np, d_map);
+        const bool vec = L % 16 == 0 && (reinterpret_cast<uintptr_t>(d_payloads) & 15) == 0 &&
+                         (reinterpret_cast<uintptr_t>(d_out) & 15) == 0;
+        if (vec)
+            copy_rows_kernel<16><<<grid_for((uint64_t)np * (L / 16), 256), 256, 0, st>>>(d_payloads, d_out, L,
+                                                                                            d_pres, np, d_map);
+        else
+            copy_rows_kernel<1><<<grid_for((uint64_t)np * L, 256), 256, 0, st>>>(d_payloads, d_out, L, d_pres, np,
+                                                                                   d_map);
         SCRS_CUDA(cudaGetLastError());
     }
     if (nm == 0) return SCRS_OK;
