@@ -211,7 +211,8 @@ __device__ __forceinline__ void store_planes(uint8_t* p, const uint32_t (&w)[16]
 }
 
 // work[i] = planes(values[i] * payload_i) for known i < n_rows_src, else 0
-// (the product evaluations of F*L, decoder.rs:320-333).
+// (the product evaluations of F*L, decoder.rs:320-333).  known == nullptr:
+// every row is known; values == nullptr: the rows are sliced unscaled.
 __global__ void __launch_bounds__(128) scale_in_kernel(const uint8_t* payloads, uint64_t L, uint32_t G,
                                                        const uint8_t* known, const uint16_t* values,
                                                        uint32_t ts, uint8_t* work, const uint16_t* row_map) {
@@ -222,12 +223,17 @@ __global__ void __launch_bounds__(128) scale_in_kernel(const uint8_t* payloads, 
         uint32_t acc[16];
 #pragma unroll
         for (int t = 0; t < 16; t++) acc[t] = 0;
-        if (known[row]) {
+        if (!known || known[row]) {
             uint32_t w[16];
             const uint64_t src = row_map ? row_map[row] : row;
             load_group_bytes(payloads + src * L, g, L, w);
             bitslice16(w);
-            mul16<false>(values[row], acc, w);
+            if (values) {
+                mul16<false>(values[row], acc, w);
+            } else {
+#pragma unroll
+                for (int t = 0; t < 16; t++) acc[t] = w[t];
+            }
         }
         store_planes(work + ((uint64_t)row * G + g) * 64, acc);
     }
@@ -258,7 +264,8 @@ __global__ void __launch_bounds__(128) derivative_kernel(const uint8_t* in, uint
     }
 }
 
-// out row dst[t] = bytes(inv(derivs[src[t]]) * work[src[t]]) (decoder.rs:348-356).
+// out row dst[t] = bytes(inv(derivs[src[t]]) * work[src[t]]) (decoder.rs:348-356);
+// derivs == nullptr: the rows are unsliced unscaled.
 __global__ void __launch_bounds__(128) scale_out_kernel(const uint8_t* work, uint32_t G, uint64_t L,
                                                         const uint16_t* rows_src, const uint16_t* rows_dst,
                                                         uint32_t count, const uint16_t* derivs,
@@ -269,13 +276,18 @@ __global__ void __launch_bounds__(128) scale_out_kernel(const uint8_t* work, uin
          x += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t t = (uint32_t)(x / G), g = (uint32_t)(x % G);
         const uint32_t src = rows_src[t];
-        const uint16_t d = derivs[src];
-        const uint16_t f = d ? exp16[(kMult - log16[d]) % kMult] : 0;
         uint32_t w[16], acc[16];
         load_planes(work + ((uint64_t)src * G + g) * 64, w);
+        if (derivs) {
+            const uint16_t d = derivs[src];
+            const uint16_t f = d ? exp16[(kMult - log16[d]) % kMult] : 0;
 #pragma unroll
-        for (int q = 0; q < 16; q++) acc[q] = 0;
-        mul16<false>(f, acc, w);
+            for (int q = 0; q < 16; q++) acc[q] = 0;
+            mul16<false>(f, acc, w);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 16; q++) acc[q] = w[q];
+        }
         bitslice16(acc);
         store_group_bytes(out + (uint64_t)rows_dst[t] * L, g, L, acc);
     }
@@ -382,8 +394,10 @@ int grid_for(uint64_t items, int threads) {
 }
 
 // Full transform of 2^D bit-sliced rows (heap root 1), forward or inverse.
+// root: heap index of the transform's root node (1: the whole transform of
+// 2^D rows; 2 and 3: the halves below it, each of 2^D rows, D one less).
 cudaError_t run_transform(uint8_t* work, uint32_t G, int D, const uint16_t* factors, bool forward,
-                          cudaStream_t st) {
+                          cudaStream_t st, uint32_t root = 1) {
     static uint64_t attr = 0;
     if (first_on_device(attr)) {
         cudaError_t e = cudaFuncSetAttribute(afft_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -418,7 +432,7 @@ cudaError_t run_transform(uint8_t* work, uint32_t G, int D, const uint16_t* fact
         // one butterfly per thread and level (a multiple of 32, at most kPassThreads)
         const uint32_t bfly = (1u << (c - 1)) * gt;
         const int threads = (int)std::min<uint32_t>(kPassThreads, std::max<uint32_t>(32, (bfly + 31) / 32 * 32));
-        afft_pass_kernel<<<tiles, threads, smem, st>>>(work, G, D, 1, l0, c, forward ? 1 : 0, factors, gt);
+        afft_pass_kernel<<<tiles, threads, smem, st>>>(work, G, D, root, l0, c, forward ? 1 : 0, factors, gt);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
@@ -657,6 +671,26 @@ int32_t AfftCodec::encode(const uint8_t* d_data, uint8_t* d_repairs, AfftWorkspa
                           cudaStream_t st, scrs_error* err) const {
     (void)status;
     const uint32_t G = (uint32_t)((L + 63) / 64);
+    if (2 * k == ts) {
+        // k a power of two (and m <= k): the data points are the left half of
+        // the transform's points and the repair points the first m of the right
+        // half.  The top butterfly level of a forward transform whose upper
+        // coefficients are zero copies the lower half into the upper, so the
+        // repairs are the right half-transform of the left half-transform's
+        // inverse of the data: two transforms of k points, no locator, no
+        // derivative (the reference encoder is this IFFT-then-forward form,
+        // afft/encoder.rs:150-250).
+        scale_in_kernel<<<grid_for(k * G, 128), 128, 0, st>>>(d_data, L, G, nullptr, nullptr, (uint32_t)k,
+                                                              ws.work0.as<uint8_t>(), nullptr);
+        SCRS_CUDA(cudaGetLastError());
+        SCRS_CUDA(run_transform(ws.work0.as<uint8_t>(), G, (int)log_ts - 1, factors.as<uint16_t>(), false, st, 2));
+        SCRS_CUDA(run_transform(ws.work0.as<uint8_t>(), G, (int)log_ts - 1, factors.as<uint16_t>(), true, st, 3));
+        scale_out_kernel<<<grid_for(m * G, 128), 128, 0, st>>>(ws.work0.as<uint8_t>(), G, L,
+                                                               ws.rows.as<uint16_t>() + m, ws.rows.as<uint16_t>() + m,
+                                                               (uint32_t)m, nullptr, nullptr, nullptr, d_repairs);
+        SCRS_CUDA(cudaGetLastError());
+        return SCRS_OK;
+    }
     const uint16_t *lg, *ex;
     SCRS_CUDA(log16_tables(&lg, &ex));
     scale_in_kernel<<<grid_for(ts * G, 128), 128, 0, st>>>(d_data, L, G, ws.known.as<uint8_t>(),
