@@ -168,10 +168,4 @@ __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
-// Bulk prefetch of [src, src + bytes) into L2 (src 16-byte aligned, bytes a
-// multiple of 16).
-__device__ __forceinline__ void prefetch_l2_bulk(const void* gmem_src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(gmem_src), "r"(bytes) : "memory");
-}
-
 }  // namespace scrs

@@ -147,8 +147,6 @@ namespace scrs {
     parts.append(asm_function("brx_mul8x2_lo",
                               "acc[0..7] ^= v*p[0..7], acc[8..15] ^= v*p[8..15] for v < 16: one 16-way jump.", 16,
                               [(list(range(16)), "v")]))
-    parts.append(asm_function("brx_mul8_lo", "acc ^= v*p for v < 16: one 16-way jump.", 8,
-                              [(list(range(16)), "v")]))
     parts.append(asm_function("brx_mul8x2_nib_div",
                               "As brx_mul8x2_nib, for coefficients that may differ across the warp.", 16,
                               [(list(range(16)), "lo"), ([v << 4 for v in range(16)], "hi")], uniform=False))
