@@ -151,6 +151,48 @@ __global__ void locator_mul_kernel(uint32_t* a, const uint32_t* b, uint32_t ts) 
         a[i] = (uint32_t)(((uint64_t)a[i] * b[i]) % kMult);
 }
 
+// The whole locator in one CTA for transforms of at most kLocatorOneCtaTs
+// points: the same steps as locator_init -> 2 WHTs -> locator_mul -> WHT ->
+// locator_finish, on shared-memory copies of both arrays (one launch instead
+// of nine; at these sizes launch gaps, not arithmetic, set the time).
+constexpr uint32_t kLocatorOneCtaTs = 16384;
+
+__device__ __forceinline__ void wht_block(uint32_t* v, uint32_t ts) {
+    for (uint32_t half = 1; half < ts; half <<= 1) {
+        for (uint32_t p = threadIdx.x; p < ts / 2; p += blockDim.x) {
+            const uint32_t i = ((p / half) * 2 * half) + (p % half);
+            const uint32_t a = v[i], b = v[i + half];
+            v[i] = add_mod(a, b);
+            v[i + half] = sub_mod(a, b);
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(1024) locator_one_cta_kernel(const uint8_t* known, uint32_t ts, uint32_t inv_size,
+                                                               const uint16_t* log16, const uint16_t* exp16,
+                                                               uint16_t* values, uint16_t* derivs) {
+    extern __shared__ uint32_t sm_loc[];
+    uint32_t* a = sm_loc;
+    uint32_t* b = sm_loc + ts;
+    for (uint32_t i = threadIdx.x; i < ts; i += blockDim.x) {
+        a[i] = known[i] ? 0u : 1u;
+        b[i] = log16[i];
+    }
+    __syncthreads();
+    wht_block(a, ts);
+    wht_block(b, ts);
+    for (uint32_t i = threadIdx.x; i < ts; i += blockDim.x) a[i] = (uint32_t)(((uint64_t)a[i] * b[i]) % kMult);
+    __syncthreads();
+    wht_block(a, ts);
+    for (uint32_t i = threadIdx.x; i < ts; i += blockDim.x) {
+        const uint32_t e = (uint32_t)(((uint64_t)a[i] * inv_size) % kMult);
+        const uint16_t prod = exp16[e];
+        values[i] = known[i] ? prod : 0;
+        derivs[i] = known[i] ? 0 : prod;
+    }
+}
+
 __global__ void locator_finish_kernel(const uint32_t* a, const uint8_t* known, uint32_t ts, uint32_t inv_size,
                                       const uint16_t* exp16, uint16_t* values, uint16_t* derivs) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ts; i += gridDim.x * blockDim.x) {
@@ -487,6 +529,22 @@ int32_t afft_locator_device(const uint8_t* d_known, uint32_t ts, uint32_t* wa, u
     SCRS_CUDA(log16_tables(&lg, &ex));
     int D = 0;
     while ((1u << D) < ts) D++;
+    if (ts <= kLocatorOneCtaTs) {
+        static uint64_t attr = 0;
+        const int smem = (int)(2 * kLocatorOneCtaTs * sizeof(uint32_t));
+        if (first_on_device(attr)) {
+            cudaError_t e = cudaFuncSetAttribute(locator_one_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 smem);
+            if (e != cudaSuccess) {
+                attr = 0;
+                SCRS_CUDA(e);
+            }
+        }
+        locator_one_cta_kernel<<<1, 1024, 2 * ts * sizeof(uint32_t), st>>>(d_known, ts, mod_pow(32768, (uint32_t)D),
+                                                                           lg, ex, values, derivs);
+        SCRS_CUDA(cudaGetLastError());
+        return SCRS_OK;
+    }
     const int g = grid_for(ts, 256);
     locator_init_kernel<<<g, 256, 0, st>>>(d_known, ts, lg, wa, wb);
     SCRS_CUDA(cudaGetLastError());
