@@ -698,10 +698,29 @@ int32_t AfftWorkspace::init_encode(const AfftCodec& c, scrs_error* err) {
     std::vector<uint8_t> hk(c.ts, 0);
     std::fill(hk.begin(), hk.begin() + c.k, 1);
     SCRS_CUDA(cudaMemcpy(known.p, hk.data(), c.ts, cudaMemcpyHostToDevice));
-    host_rows.resize(2 * c.m);
+    std::vector<uint16_t> host_rows(2 * c.m);
     for (uint64_t t = 0; t < c.m; t++) host_rows[t] = (uint16_t)(c.k + t), host_rows[c.m + t] = (uint16_t)t;
     SCRS_CUDA(rows.ensure(host_rows.size() * 2));
     SCRS_CUDA(cudaMemcpy(rows.p, host_rows.data(), host_rows.size() * 2, cudaMemcpyHostToDevice));
+    return SCRS_OK;
+}
+
+AfftWorkspace::~AfftWorkspace() {
+    if (staged) {
+        if (stage_pending) cudaEventSynchronize(staged);  // copies still reading `stage`
+        cudaEventDestroy(staged);
+    }
+}
+
+int32_t AfftWorkspace::stage_acquire(scrs_error* err) {
+    if (stage_pending) SCRS_CUDA(cudaEventSynchronize(staged));
+    stage_pending = false;
+    return SCRS_OK;
+}
+
+int32_t AfftWorkspace::stage_release(cudaStream_t st, scrs_error* err) {
+    SCRS_CUDA(cudaEventRecord(staged, st));
+    stage_pending = true;
     return SCRS_OK;
 }
 
@@ -716,9 +735,15 @@ int32_t AfftWorkspace::init_decode(const AfftCodec& c, scrs_error* err) {
     SCRS_CUDA(values.ensure(c.ts * 2));
     SCRS_CUDA(derivs.ensure(c.ts * 2));
     SCRS_CUDA(row_map.ensure(c.n * 2));
-    host_known.assign(c.ts, 0);
-    host_rows.assign(2 * c.k + 8, 0);
-    SCRS_CUDA(rows.ensure(host_rows.size() * 2));
+    const size_t rows_bytes = (2 * c.k + 8) * 2;
+    const size_t lists_elems = 3 * c.k + 4 * kTargetedMax + kTargetedMax * kTargetedMax + 8;
+    off_map = (rows_bytes + 15) & ~(size_t)15;
+    off_known = (off_map + c.n * 2 + 15) & ~(size_t)15;
+    off_lists = (off_known + c.ts + 15) & ~(size_t)15;
+    SCRS_CUDA(stage.ensure(off_lists + lists_elems * 2));
+    memset(stage.p, 0, stage.bytes);
+    if (!staged) SCRS_CUDA(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
+    SCRS_CUDA(rows.ensure(rows_bytes));
     SCRS_CUDA(tgen.ensure(kTargetedMax * c.k * 2));
     SCRS_CUDA(tcoef.ensure(kTargetedMax * c.k * 2));
     SCRS_CUDA(tlists.ensure((3 * c.k + 4 * kTargetedMax + kTargetedMax * kTargetedMax + 8) * 2));
@@ -776,8 +801,11 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
     const uint16_t *lg, *ex;
     SCRS_CUDA(log16_tables(&lg, &ex));
     // missing data rows (afft/decoder.rs:276-286) and present data rows
-    uint16_t* miss = ws.host_rows.data();
-    uint16_t* pres = ws.host_rows.data() + k;
+    int32_t rc = ws.stage_acquire(err);
+    if (rc) return rc;
+    uint8_t* stage = ws.stage.as<uint8_t>();
+    uint16_t* miss = reinterpret_cast<uint16_t*>(stage);
+    uint16_t* pres = miss + k;
     uint32_t nm = 0, np = 0;
     for (uint64_t d = 0; d < k; d++) {
         if (have[d])
@@ -785,12 +813,13 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
         else
             miss[nm++] = (uint16_t)d;
     }
-    SCRS_CUDA(cudaMemcpyAsync(ws.rows.p, ws.host_rows.data(), ws.host_rows.size() * 2, cudaMemcpyHostToDevice, st));
+    SCRS_CUDA(cudaMemcpyAsync(ws.rows.p, miss, (2 * k + 8) * 2, cudaMemcpyHostToDevice, st));
     const uint16_t* d_miss = ws.rows.as<uint16_t>();
     const uint16_t* d_pres = ws.rows.as<uint16_t>() + k;
     const uint16_t* d_map = nullptr;
     if (row_map) {
-        SCRS_CUDA(cudaMemcpyAsync(ws.row_map.p, row_map, n * 2, cudaMemcpyHostToDevice, st));
+        memcpy(stage + ws.off_map, row_map, n * 2);
+        SCRS_CUDA(cudaMemcpyAsync(ws.row_map.p, stage + ws.off_map, n * 2, cudaMemcpyHostToDevice, st));
         d_map = ws.row_map.as<uint16_t>();
     }
     if (np) {
@@ -804,11 +833,17 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
                                                                                    d_map);
         SCRS_CUDA(cudaGetLastError());
     }
-    if (nm == 0) return SCRS_OK;
-    if (nm <= kTargetedMax) return decode_targeted(d_payloads, have, d_out, ws, status, st, err, row_map, miss, nm,
-                                                   pres, np);
-    for (uint64_t i = 0; i < ts; i++) ws.host_known[i] = (i < n && have[i]) ? 1 : 0;
-    SCRS_CUDA(cudaMemcpyAsync(ws.known.p, ws.host_known.data(), ts, cudaMemcpyHostToDevice, st));
+    if (nm == 0) return ws.stage_release(st, err);
+    if (nm <= kTargetedMax) {
+        rc = decode_targeted(d_payloads, have, d_out, ws, status, st, err, row_map, miss, nm, pres, np);
+        const int32_t rr = ws.stage_release(st, err);  // after its list upload, on every path
+        return rc ? rc : rr;
+    }
+    uint8_t* known = stage + ws.off_known;
+    for (uint64_t i = 0; i < ts; i++) known[i] = (i < n && have[i]) ? 1 : 0;
+    SCRS_CUDA(cudaMemcpyAsync(ws.known.p, known, ts, cudaMemcpyHostToDevice, st));
+    rc = ws.stage_release(st, err);
+    if (rc) return rc;
     int32_t r = afft_locator_device(ws.known.as<uint8_t>(), (uint32_t)ts, ws.wht_a.as<uint32_t>(),
                                     ws.wht_b.as<uint32_t>(), ws.values.as<uint16_t>(), ws.derivs.as<uint16_t>(), st,
                                     err);
@@ -838,8 +873,9 @@ int32_t AfftCodec::decode_targeted(const uint8_t* d_payloads, const uint8_t* hav
     SCRS_CUDA(log16_tables(&lg, &ex));
     // lists: in_rows[k] (repairs then present), out_rows[nm], rep[nm] (evaluation points),
     // missing[nm], present[np]
-    std::vector<uint16_t> h(3 * k + 4 * kTargetedMax + kTargetedMax * kTargetedMax + 8, 0);
-    uint16_t* in_rows = h.data();
+    const size_t n_lists = 3 * k + 4 * kTargetedMax + kTargetedMax * kTargetedMax + 8;
+    uint16_t* h = reinterpret_cast<uint16_t*>(ws.stage.as<uint8_t>() + ws.off_lists);  // acquired by decode()
+    uint16_t* in_rows = h;
     uint16_t* out_rows = in_rows + k;
     uint16_t* rep = out_rows + kTargetedMax;
     uint16_t* mis = rep + kTargetedMax;
@@ -851,7 +887,7 @@ int32_t AfftCodec::decode_targeted(const uint8_t* d_payloads, const uint8_t* hav
     auto payload_row = [&](uint32_t w) { return row_map ? row_map[w] : (uint16_t)w; };
     for (uint32_t t = 0; t < nm; t++) in_rows[t] = payload_row(rep[t]), out_rows[t] = miss[t], mis[t] = miss[t];
     for (uint32_t z = 0; z < np; z++) in_rows[nm + z] = payload_row(pres[z]), prs[z] = pres[z];
-    SCRS_CUDA(cudaMemcpyAsync(ws.tlists.p, h.data(), h.size() * 2, cudaMemcpyHostToDevice, st));
+    SCRS_CUDA(cudaMemcpyAsync(ws.tlists.p, h, n_lists * 2, cudaMemcpyHostToDevice, st));
     const uint16_t* d_in_rows = ws.tlists.as<uint16_t>();
     const uint16_t* d_out_rows = d_in_rows + k;
     const uint16_t* d_rep = d_out_rows + kTargetedMax;

@@ -50,8 +50,22 @@ class AfftCodec {
 
 class AfftWorkspace {
    public:
+    AfftWorkspace() = default;
+    AfftWorkspace(const AfftWorkspace&) = delete;
+    AfftWorkspace& operator=(const AfftWorkspace&) = delete;
+    ~AfftWorkspace();
     int32_t init_encode(const AfftCodec& c, scrs_error* err);
     int32_t init_decode(const AfftCodec& c, scrs_error* err);
+    // Host side of a decode's uploads (row lists, codeword -> payload row map,
+    // known-point mask, targeted lists) in pinned memory, so the copies are
+    // asynchronous; the next decode waits for the previous one's copies
+    // before it rewrites the area.
+    int32_t stage_acquire(scrs_error* err);
+    int32_t stage_release(cudaStream_t st, scrs_error* err);
+    PinnedBuf stage;
+    cudaEvent_t staged = nullptr;
+    bool stage_pending = false;
+    size_t off_map = 0, off_known = 0, off_lists = 0;  // byte offsets in `stage` (rows at 0)
     DevBuf work0, work1;            // ts * L bytes, bit-sliced rows
     DevBuf known;                   // uint8[ts]
     DevBuf wht_a, wht_b;            // uint32[ts]
@@ -59,8 +73,6 @@ class AfftWorkspace {
     DevBuf rows;                    // uint16 lists for the output stage
     DevBuf row_map;                 // uint16[n] codeword index -> payload row
     DevBuf tgen, tcoef, tlists;     // targeted decode: generator rows, fused coefficients, lists
-    std::vector<uint8_t> host_known;
-    std::vector<uint16_t> host_rows;
     uint64_t k = 0, m = 0, L = 0;
 };
 

@@ -453,6 +453,8 @@ struct scrs_decode_scratch {
     RecipeBufs recipe;
     DevBuf d_out;  // k * L: host finalize lands here before the copy back
     std::unique_ptr<AfftWorkspace> afft;
+    // per-call index lists, capacity reserved at creation (no allocation per call)
+    std::vector<uint16_t> missing, present, repairs;
 };
 
 extern "C" int32_t scrs_decoder_create(const scrs_profile* p, scrs_decoder** out, scrs_error* err) {
@@ -500,6 +502,9 @@ extern "C" int32_t scrs_decoder_scratch(const scrs_decoder* d, scrs_decode_scrat
     s->kind = d->p.engine;
     s->p = d->p;
     const uint32_t k = (uint32_t)d->p.k, m = (uint32_t)d->p.m;
+    s->missing.reserve(k);
+    s->present.reserve(k);
+    s->repairs.reserve(m);
     if (d->afft) {
         s->afft.reset(new (std::nothrow) AfftWorkspace());
         if (!s->afft) return set_err(err, SCRS_ERR_OUT_OF_MEMORY, sizeof(AfftWorkspace));
@@ -588,7 +593,10 @@ int32_t finalize_device(scrs_decoder* d, uint8_t* d_out, scrs_decode_scratch* s,
     if (d->afft) return d->afft->decode(d->payloads.as<uint8_t>(), d->have.data(), d_out, *s->afft,
                                         d->status.dev, st, err);
     // build_recipe (decoder/streaming.rs:163-194, tower/decoder.rs:218-247)
-    std::vector<uint16_t> missing, present, repairs;
+    std::vector<uint16_t>&missing = s->missing, &present = s->present, &repairs = s->repairs;
+    missing.clear();
+    present.clear();
+    repairs.clear();
     for (uint32_t i = 0; i < k; i++) (d->have[i] ? present : missing).push_back((uint16_t)i);
     for (uint32_t j = 0; j < m && repairs.size() < missing.size(); j++)
         if (d->have[k + j]) repairs.push_back((uint16_t)j);
@@ -702,6 +710,9 @@ struct scrs_batch_decode_scratch {
     DevBuf d_rows, d_out;       // received rows / output (GF(256) host path)
     PinnedBuf h_rows;
     scrs_decode_scratch* lazy = nullptr;  // GF(65536)
+    // per-call index lists, their capacity reserved here so that the calls
+    // allocate nothing
+    std::vector<uint16_t> missing, present, repairs, row_of;
     ~scrs_batch_decode_scratch() { scrs_decode_scratch_destroy(lazy); }
 };
 
@@ -739,6 +750,10 @@ extern "C" int32_t scrs_batch_decoder_scratch(const scrs_batch_decoder* b, scrs_
     s->p = b->p;
     const uint32_t k = (uint32_t)b->p.k, m = (uint32_t)b->p.m;
     const uint64_t L = b->p.symbol_len;
+    s->missing.reserve(k);
+    s->present.reserve(k);
+    s->repairs.reserve(m);
+    s->row_of.reserve((size_t)k + m);
     if (b->lazy) {
         int32_t st = scrs_decoder_scratch(b->lazy, &s->lazy, err);
         if (st) return st;
@@ -770,6 +785,9 @@ int32_t gf8_batch_validate(const scrs_batch_decoder* b, const uint64_t* idx, con
     if (count && !idx) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
     uint8_t seen[256] = {0};
     row_of.assign(n, kNoRow);
+    missing.clear();
+    present.clear();
+    repairs.clear();
     for (uint64_t q = 0; q < count; q++) {
         uint64_t i = idx[q];
         if (i >= n) return set_err(err, SCRS_DECODE_INDEX_OUT_OF_RANGE, i, n);
@@ -816,8 +834,7 @@ extern "C" int32_t scrs_batch_decode_into_with(scrs_batch_decoder* b, const uint
         return scrs_dec_finalize_into_with(b->lazy, out, out_len, s->lazy, err);
     }
     if (s->lazy) return set_err(err, SCRS_DECODE_SCRATCH_MISMATCH);
-    std::vector<uint16_t> missing, present, repairs, row_of;
-    int32_t r = gf8_batch_validate(b, idx, lens, count, out_len, s, missing, present, repairs, row_of, err);
+    int32_t r = gf8_batch_validate(b, idx, lens, count, out_len, s, s->missing, s->present, s->repairs, s->row_of, err);
     if (r) return r;
     if (!out || (count && !pay)) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
     const uint64_t L = b->p.symbol_len;
@@ -825,7 +842,7 @@ extern "C" int32_t scrs_batch_decode_into_with(scrs_batch_decoder* b, const uint
     for (uint64_t q = 0; q < count; q++) memcpy(h + q * L, pay[q], L);
     cudaStream_t st = b->stream.s;
     SCRS_CUDA(cudaMemcpyAsync(s->d_rows.p, h, count * L, cudaMemcpyHostToDevice, st));
-    r = gf8_batch_run(b, missing, present, repairs, row_of, s->d_rows.as<uint8_t>(), s->d_out.as<uint8_t>(), s,
+    r = gf8_batch_run(b, s->missing, s->present, s->repairs, s->row_of, s->d_rows.as<uint8_t>(), s->d_out.as<uint8_t>(), s,
                       st, err);
     if (r) return r;
     SCRS_CUDA(cudaMemcpyAsync(out, s->d_out.p, out_len, cudaMemcpyDeviceToHost, st));
@@ -863,7 +880,8 @@ extern "C" int32_t scrs_batch_decode_into_with_device(scrs_batch_decoder* b, con
         if (count && (!idx || !d_rows)) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
         scrs_decoder* d = b->lazy;
         scrs_dec_reset(d);
-        std::vector<uint16_t> row_of(n, kNoRow);
+        std::vector<uint16_t>& row_of = s->row_of;
+        row_of.assign(n, kNoRow);
         for (uint64_t q = 0; q < count; q++) {
             if (idx[q] >= n) return set_err(err, SCRS_DECODE_INDEX_OUT_OF_RANGE, idx[q], n);
             if (row_of[idx[q]] != kNoRow) return set_err(err, SCRS_DECODE_DUPLICATE_INDEX, idx[q]);
@@ -878,7 +896,10 @@ extern "C" int32_t scrs_batch_decode_into_with_device(scrs_batch_decoder* b, con
             r = d->afft->decode(d_rows, d->have.data(), d_out, *s->lazy->afft, d->status.dev, st, err,
                                 row_of.data());
         } else {
-            std::vector<uint16_t> missing, present, repairs;
+            std::vector<uint16_t>&missing = s->missing, &present = s->present, &repairs = s->repairs;
+            missing.clear();
+            present.clear();
+            repairs.clear();
             for (uint32_t i = 0; i < k; i++) (d->have[i] ? present : missing).push_back((uint16_t)i);
             for (uint32_t j = 0; j < b->p.m && repairs.size() < missing.size(); j++)
                 if (d->have[k + j]) repairs.push_back((uint16_t)j);
@@ -891,11 +912,11 @@ extern "C" int32_t scrs_batch_decode_into_with_device(scrs_batch_decoder* b, con
         return set_err(err, SCRS_OK);
     }
     if (s->lazy) return set_err(err, SCRS_DECODE_SCRATCH_MISMATCH);
-    std::vector<uint16_t> missing, present, repairs, row_of;
-    int32_t r = gf8_batch_validate(b, idx, nullptr, count, out_len, s, missing, present, repairs, row_of, err);
+    int32_t r = gf8_batch_validate(b, idx, nullptr, count, out_len, s, s->missing, s->present, s->repairs, s->row_of,
+                                   err);
     if (r) return r;
     if (!d_out || (count && !d_rows)) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
-    r = gf8_batch_run(b, missing, present, repairs, row_of, d_rows, d_out, s, st, err);
+    r = gf8_batch_run(b, s->missing, s->present, s->repairs, s->row_of, d_rows, d_out, s, st, err);
     if (r) return r;
     return set_err(err, SCRS_OK);
 }
