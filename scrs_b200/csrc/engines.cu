@@ -67,12 +67,14 @@ struct RecipeBufs {
     DevBuf lists;   // uint16: in_rows[k] pass_rows[k] out_rows[rmax] missing[rmax] repairs[rmax] present[k]
     DevBuf work;    // uint32[4*rmax] when rmax exceeds the shared-memory plan limit
     std::vector<uint16_t> host;  // same layout as `lists`
+    std::vector<uint16_t> probe; // the key being looked up (capacity reserved at init)
     std::vector<std::unique_ptr<Entry>> cache;
     uint64_t clock = 0, hits = 0;
     uint32_t k = 0, rmax = 0, elem = 1;
     cudaError_t init(uint32_t k_, uint32_t rmax_, uint32_t elem_) {
         k = k_, rmax = rmax_, elem = elem_;
         host.assign((size_t)3 * k + 3 * rmax + 8, 0);
+        probe.reserve(1 + 2 * (size_t)rmax);
         cudaError_t e = lists.ensure(host.size() * sizeof(uint16_t));
         if (e == cudaSuccess && rmax > kPlanSmemMaxR) e = work.ensure((size_t)4 * rmax * sizeof(uint32_t));
         return e;
@@ -81,8 +83,8 @@ struct RecipeBufs {
     // (re)computed.  The least recently used entry is reused when full.
     cudaError_t lookup(const std::vector<uint16_t>& missing, const std::vector<uint16_t>& repairs, void** coef,
                        bool* fresh) {
-        std::vector<uint16_t> key;
-        key.reserve(1 + missing.size() + repairs.size());
+        std::vector<uint16_t>& key = probe;
+        key.clear();
         key.push_back((uint16_t)missing.size());
         key.insert(key.end(), missing.begin(), missing.end());
         key.insert(key.end(), repairs.begin(), repairs.end());
@@ -119,7 +121,7 @@ struct RecipeBufs {
             slot->key.clear();
             return e;
         }
-        slot->key = std::move(key);
+        slot->key.assign(key.begin(), key.end());
         slot->last_use = ++clock;
         *coef = slot->coef.p;
         *fresh = true;
@@ -445,6 +447,10 @@ struct scrs_decoder {
     uint64_t distinct = 0, received = 0;
     TowerTables tower;
     std::unique_ptr<AfftCodec> afft;
+    cudaEvent_t uploaded = nullptr;  // orders the payload uploads before a caller's stream
+    ~scrs_decoder() {
+        if (uploaded) cudaEventDestroy(uploaded);
+    }
 };
 
 struct scrs_decode_scratch {
@@ -467,6 +473,7 @@ extern "C" int32_t scrs_decoder_create(const scrs_profile* p, scrs_decoder** out
     const uint64_t n = p->k + p->m, L = p->symbol_len;
     SCRS_CUDA(d->stream.init());
     SCRS_CUDA(d->status.init());
+    SCRS_CUDA(cudaEventCreateWithFlags(&d->uploaded, cudaEventDisableTiming));
     SCRS_CUDA(d->payloads.ensure(n * L));
     SCRS_CUDA(d->staging.ensure(n * L));
     d->have.assign(n, 0);
@@ -584,11 +591,8 @@ int32_t finalize_device(scrs_decoder* d, uint8_t* d_out, scrs_decode_scratch* s,
     int32_t r = upload_staged(d, err);
     if (r) return r;
     if (st != d->stream.s) {  // order the payload uploads before the caller's stream
-        cudaEvent_t ev;
-        SCRS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        cudaEventRecord(ev, d->stream.s);
-        cudaStreamWaitEvent(st, ev, 0);
-        cudaEventDestroy(ev);
+        SCRS_CUDA(cudaEventRecord(d->uploaded, d->stream.s));
+        SCRS_CUDA(cudaStreamWaitEvent(st, d->uploaded, 0));
     }
     if (d->afft) return d->afft->decode(d->payloads.as<uint8_t>(), d->have.data(), d_out, *s->afft,
                                         d->status.dev, st, err);
