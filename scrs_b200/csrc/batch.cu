@@ -207,14 +207,20 @@ int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc
             T.n_out = d.m;
             T.ld = d.m;
         } else {
+            // k + m <= 256 (validated above): fixed-size lists, no allocation per stripe
             const uint32_t k = d.k, n = d.k + d.m;
-            std::vector<uint16_t> row_of(n, kNoRow);
+            uint16_t row_of[256], missing[256], present[256], repairs[256];
+            std::fill(row_of, row_of + n, kNoRow);
             for (uint32_t q = 0; q < k; q++) row_of[d.indices[q]] = (uint16_t)q;
-            std::vector<uint16_t> missing, present, repairs;
-            for (uint32_t i = 0; i < k; i++) (row_of[i] != kNoRow ? present : missing).push_back((uint16_t)i);
+            uint32_t r = 0, p = 0, nrep = 0;
+            for (uint32_t i = 0; i < k; i++) {
+                if (row_of[i] != kNoRow)
+                    present[p++] = (uint16_t)i;
+                else
+                    missing[r++] = (uint16_t)i;
+            }
             for (uint32_t j = 0; j < d.m; j++)
-                if (row_of[k + j] != kNoRow) repairs.push_back((uint16_t)j);
-            const uint32_t r = (uint32_t)missing.size(), p = (uint32_t)present.size();
+                if (row_of[k + j] != kNoRow) repairs[nrep++] = (uint16_t)j;
             uint16_t* L16 = reinterpret_cast<uint16_t*>(b->arena.data() + off);
             uint16_t* in_rows = L16;
             uint16_t* pass_rows = L16 + k;
@@ -224,10 +230,10 @@ int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc
             uint16_t* l_present = l_repairs + r;
             for (uint32_t t = 0; t < r; t++) in_rows[t] = row_of[k + repairs[t]], pass_rows[t] = kNoRow;
             for (uint32_t z = 0; z < p; z++) in_rows[r + z] = row_of[present[z]], pass_rows[r + z] = present[z];
-            std::copy(missing.begin(), missing.end(), out_rows);
-            std::copy(missing.begin(), missing.end(), l_missing);
-            std::copy(repairs.begin(), repairs.end(), l_repairs);
-            std::copy(present.begin(), present.end(), l_present);
+            std::copy(missing, missing + r, out_rows);
+            std::copy(missing, missing + r, l_missing);
+            std::copy(repairs, repairs + nrep, l_repairs);
+            std::copy(present, present + p, l_present);
             const size_t dl = (size_t)(reinterpret_cast<uint8_t*>(L16) - b->arena.data());
             uint16_t* dL16 = reinterpret_cast<uint16_t*>(dbase + dl);
             off = align16(off + 2 * ((size_t)3 * k + 3 * r));

@@ -68,3 +68,20 @@ def test_specialised_cfg1_geometry_with_decodes(gpu, oracle):
     b.set(stripes)
     assert b.jit_stripes == 700
     run_and_check(torch, b, outs, expect, graph=True)
+
+
+def test_specialised_widest_geometries(gpu, oracle):
+    """The largest staged row count (k = 32) and the largest product count
+    (k * m = 64) a specialised kernel takes."""
+    torch = pytest.importorskip("torch")
+    from scrs_b200.batch import StripeBatch
+
+    rng = np.random.default_rng(41)
+    specs = [(OP_ENCODE, Engine.GOOD_CAUCHY, 32, 2, 4096)] * 600
+    specs += [(OP_ENCODE, Engine.STANDARD_CAUCHY, 16, 4, 2048)] * 1200
+    stripes, outs, expect, keep = device_stripes(torch, oracle, specs, rng)
+    b = StripeBatch(gpu.lib, len(stripes))
+    b.set(stripes)
+    assert b.jit_stripes == 1800
+    run_and_check(torch, b, outs, expect, graph=False)
+
