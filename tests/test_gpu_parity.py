@@ -138,7 +138,7 @@ def test_lazy_decoder_push_contract_matches_oracle(gpu, oracle):
 # ---------------------------------------------------------------- tower
 
 @pytest.mark.parametrize("k,m,L", [(4, 3, 10), (4, 3, 18), (32, 8, 65536), (64, 32, 66), (256, 3, 4),
-                                   (300, 20, 130), (2, 1, 4)])
+                                   (300, 20, 130), (2, 1, 4), (2048, 512, 16)])
 def test_tower_encode_matches_oracle(gpu, oracle, k, m, L):
     p = gpu.resolve(Engine.TOWER, k, m, L)
     data = gfpy.rng_bytes(k * L, 11 * k + m)
@@ -178,7 +178,7 @@ def test_tower_cfg2_shape(gpu, oracle):
 
 @pytest.mark.parametrize("k,m,L", [(5, 3, 6), (8, 4, 64), (3, 2, 2), (100, 20, 64), (17, 7, 130), (4, 2, 64),
                                    (16, 4, 40), (256, 64, 48), (512, 128, 40), (1, 1, 2), (8, 8, 4),
-                                   (4096, 4096, 1024)])
+                                   (4096, 4096, 1024), (32768, 32768, 4), (40000, 25536, 2)])
 def test_afft_encode_matches_oracle(gpu, oracle, k, m, L):
     p = gpu.resolve(Engine.AFFT, k, m, L)
     data = gfpy.rng_bytes(k * L, 17 * k + m)
