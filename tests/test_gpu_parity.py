@@ -25,7 +25,7 @@ def words_equal(a, b):
 @pytest.mark.parametrize("k,m,L", [(1, 1, 2), (4, 2, 16), (8, 4, 64), (10, 4, 4096), (16, 8, 1024),
                                    (32, 16, 1024), (64, 16, 4096), (128, 64, 1024), (200, 50, 256),
                                    (1, 254, 64), (254, 1, 64), (3, 5, 7), (6, 6, 33), (16, 8, 100),
-                                   (10, 4, 1000), (40, 16, 65536), (33, 3, 1025)])
+                                   (10, 4, 1000), (40, 16, 65536), (33, 3, 1025), (200, 56, 256)])
 def test_gf256_encode_matches_oracle(gpu, oracle, engine, k, m, L):
     if engine == Engine.GOOD_CAUCHY and k + m > 255:
         pytest.skip("Good Cauchy capacity is 255")
@@ -55,7 +55,7 @@ def test_gf256_all_subsets(gpu, oracle, engine, k, m, L):
 
 
 @pytest.mark.parametrize("k,m,L", [(1, 1, 2), (4, 2, 16), (8, 4, 64), (6, 6, 33), (16, 8, 100), (32, 16, 64),
-                                   (10, 4, 4096), (64, 16, 1024), (128, 127, 96)])
+                                   (10, 4, 4096), (64, 16, 1024), (128, 127, 96), (128, 128, 96)])
 def test_gf256_decode_sampled_patterns(gpu, k, m, L):
     for engine in GF256:
         if engine == Engine.GOOD_CAUCHY and k + m > 255:
