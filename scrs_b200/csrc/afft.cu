@@ -706,21 +706,23 @@ int32_t AfftWorkspace::init_encode(const AfftCodec& c, scrs_error* err) {
 }
 
 AfftWorkspace::~AfftWorkspace() {
-    if (staged) {
-        if (stage_pending) cudaEventSynchronize(staged);  // copies still reading `stage`
-        cudaEventDestroy(staged);
+    for (int i = 0; i < 2; i++) {
+        if (!staged[i]) continue;
+        if (stage_pending[i]) cudaEventSynchronize(staged[i]);  // copies still reading the area
+        cudaEventDestroy(staged[i]);
     }
 }
 
 int32_t AfftWorkspace::stage_acquire(scrs_error* err) {
-    if (stage_pending) SCRS_CUDA(cudaEventSynchronize(staged));
-    stage_pending = false;
+    cur ^= 1;
+    if (stage_pending[cur]) SCRS_CUDA(cudaEventSynchronize(staged[cur]));
+    stage_pending[cur] = false;
     return SCRS_OK;
 }
 
 int32_t AfftWorkspace::stage_release(cudaStream_t st, scrs_error* err) {
-    SCRS_CUDA(cudaEventRecord(staged, st));
-    stage_pending = true;
+    SCRS_CUDA(cudaEventRecord(staged[cur], st));
+    stage_pending[cur] = true;
     return SCRS_OK;
 }
 
@@ -740,9 +742,11 @@ int32_t AfftWorkspace::init_decode(const AfftCodec& c, scrs_error* err) {
     off_map = (rows_bytes + 15) & ~(size_t)15;
     off_known = (off_map + c.n * 2 + 15) & ~(size_t)15;
     off_lists = (off_known + c.ts + 15) & ~(size_t)15;
-    SCRS_CUDA(stage.ensure(off_lists + lists_elems * 2));
-    memset(stage.p, 0, stage.bytes);
-    if (!staged) SCRS_CUDA(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
+    for (int i = 0; i < 2; i++) {
+        SCRS_CUDA(stage[i].ensure(off_lists + lists_elems * 2));
+        memset(stage[i].p, 0, stage[i].bytes);
+        if (!staged[i]) SCRS_CUDA(cudaEventCreateWithFlags(&staged[i], cudaEventDisableTiming));
+    }
     SCRS_CUDA(rows.ensure(rows_bytes));
     SCRS_CUDA(tgen.ensure(kTargetedMax * c.k * 2));
     SCRS_CUDA(tcoef.ensure(kTargetedMax * c.k * 2));
@@ -803,7 +807,7 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
     // missing data rows (afft/decoder.rs:276-286) and present data rows
     int32_t rc = ws.stage_acquire(err);
     if (rc) return rc;
-    uint8_t* stage = ws.stage.as<uint8_t>();
+    uint8_t* stage = ws.stage_ptr();
     uint16_t* miss = reinterpret_cast<uint16_t*>(stage);
     uint16_t* pres = miss + k;
     uint32_t nm = 0, np = 0;
@@ -840,7 +844,8 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
         return rc ? rc : rr;
     }
     uint8_t* known = stage + ws.off_known;
-    for (uint64_t i = 0; i < ts; i++) known[i] = (i < n && have[i]) ? 1 : 0;
+    memcpy(known, have, n);  // receipt flags are 0 / 1
+    memset(known + n, 0, ts - n);
     SCRS_CUDA(cudaMemcpyAsync(ws.known.p, known, ts, cudaMemcpyHostToDevice, st));
     rc = ws.stage_release(st, err);
     if (rc) return rc;
@@ -874,7 +879,7 @@ int32_t AfftCodec::decode_targeted(const uint8_t* d_payloads, const uint8_t* hav
     // lists: in_rows[k] (repairs then present), out_rows[nm], rep[nm] (evaluation points),
     // missing[nm], present[np]
     const size_t n_lists = 3 * k + 4 * kTargetedMax + kTargetedMax * kTargetedMax + 8;
-    uint16_t* h = reinterpret_cast<uint16_t*>(ws.stage.as<uint8_t>() + ws.off_lists);  // acquired by decode()
+    uint16_t* h = reinterpret_cast<uint16_t*>(ws.stage_ptr() + ws.off_lists);  // acquired by decode()
     uint16_t* in_rows = h;
     uint16_t* out_rows = in_rows + k;
     uint16_t* rep = out_rows + kTargetedMax;

@@ -58,14 +58,16 @@ class AfftWorkspace {
     int32_t init_decode(const AfftCodec& c, scrs_error* err);
     // Host side of a decode's uploads (row lists, codeword -> payload row map,
     // known-point mask, targeted lists) in pinned memory, so the copies are
-    // asynchronous; the next decode waits for the previous one's copies
-    // before it rewrites the area.
+    // asynchronous.  Two areas used in turn: a decode waits only for the
+    // copies of the decode before the previous one before it rewrites an area.
     int32_t stage_acquire(scrs_error* err);
     int32_t stage_release(cudaStream_t st, scrs_error* err);
-    PinnedBuf stage;
-    cudaEvent_t staged = nullptr;
-    bool stage_pending = false;
-    size_t off_map = 0, off_known = 0, off_lists = 0;  // byte offsets in `stage` (rows at 0)
+    uint8_t* stage_ptr() const { return stage[cur].as<uint8_t>(); }
+    PinnedBuf stage[2];
+    cudaEvent_t staged[2] = {nullptr, nullptr};
+    bool stage_pending[2] = {false, false};
+    int cur = 0;
+    size_t off_map = 0, off_known = 0, off_lists = 0;  // byte offsets in an area (rows at 0)
     DevBuf work0, work1;            // ts * L bytes, bit-sliced rows
     DevBuf known;                   // uint8[ts]
     DevBuf wht_a, wht_b;            // uint32[ts]
