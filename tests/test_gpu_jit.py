@@ -85,3 +85,22 @@ def test_specialised_widest_geometries(gpu, oracle):
     assert b.jit_stripes == 1800
     run_and_check(torch, b, outs, expect, graph=False)
 
+
+
+def test_more_groups_than_specialised_runs(gpu, oracle):
+    """Five eligible encode groups, each large enough: four get specialised
+    kernels, the fifth runs on the generic drain; every output is exact."""
+    torch = pytest.importorskip("torch")
+    from scrs_b200.batch import StripeBatch
+
+    rng = np.random.default_rng(43)
+    geoms = [(Engine.GOOD_CAUCHY, 3, 2), (Engine.GOOD_CAUCHY, 4, 3), (Engine.STANDARD_CAUCHY, 5, 2),
+             (Engine.STANDARD_CAUCHY, 2, 4), (Engine.GOOD_CAUCHY, 6, 1)]
+    specs = [(OP_ENCODE, e, k, m, 4096) for e, k, m in geoms for _ in range(600)]
+    specs = [specs[i] for i in rng.permutation(len(specs))]
+    stripes, outs, expect, keep = device_stripes(torch, oracle, specs, rng)
+    b = StripeBatch(gpu.lib, len(stripes))
+    b.set(stripes)
+    assert b.jit_stripes == 4 * 600
+    run_and_check(torch, b, outs, expect, graph=True)
+    assert b.last_launches == 5  # four specialised drains and the generic drain (no decodes, no plan)
