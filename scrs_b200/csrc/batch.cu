@@ -86,8 +86,9 @@ struct scrs_stripe_batch {
 namespace {
 constexpr size_t kMaxPieces = 16;  // one work counter each in d_counter
 constexpr size_t kMaxSpecRuns = 4;  // specialised groups per batch (counters 1..4)
-// A group is specialised when it has at least one persistent grid of items.
-constexpr uint64_t kJitMinItems = 8 * 148;
+// A group is specialised when it has at least one persistent grid of items
+// (this many CTAs per SM on every SM).
+constexpr uint64_t kJitMinCtasPerSm = 8;
 }
 
 extern "C" int32_t scrs_stripe_batch_create(uint64_t max_stripes, uint64_t max_items, scrs_stripe_batch** out,
@@ -291,7 +292,7 @@ int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc
             for (uint32_t t : g) n += b->tasks[t].n_items;
             JitKernel jk{};
             scrs_error je{};
-            if (n < kJitMinItems ||
+            if (n < kJitMinCtasPerSm * (uint64_t)b->sm_count ||
                 jit_kernel(std::get<0>(key), std::get<1>(key), std::get<2>(key), true, &jk, &je) != SCRS_OK)
                 continue;  // too small to fill the GPU, or not compiled: the generic drain runs it
             const uint32_t lo = next;
