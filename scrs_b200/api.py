@@ -483,11 +483,19 @@ class IncrementalEncoder(_Handle):
     _destroy = "incremental_encoder_destroy"
 
     def feed(self, index: int, data):
-        err = _Error()
         if _is_cuda_tensor(data):
-            p, ln = _device_view(data)
-            self._lib.check(self._lib.inc_feed_device(self._ptr, index, p, ln, C.byref(err)), err)
-            return
+            # per-symbol hot path: one error struct per handle, no temporaries
+            if data.is_contiguous():
+                errs = self.__dict__.get("_errs")
+                if errs is None:
+                    e = _Error()
+                    errs = self._errs = (e, C.byref(e))
+                st = self._lib.inc_feed_device(self._ptr, index, data.data_ptr(), data.nbytes, errs[1])
+                if st:
+                    self._lib.check(st, errs[0])
+                return
+            raise ValueError("device buffer must be contiguous")
+        err = _Error()
         p, ln, keep = _host_view(data)
         self._lib.check(self._lib.inc_feed(self._ptr, index, p, ln, C.byref(err)), err)
 
@@ -520,14 +528,22 @@ class Decoder(_Handle):
         return DecodeScratch(self._lib, out, self.profile)
 
     def push(self, index: int, payload) -> PushOutcome:
-        err, o = _Error(), _Push()
         if _is_cuda_tensor(payload):
-            p, ln = _device_view(payload)
-            st = self._lib.dec_push_device(self._ptr, index, p, ln, C.byref(o), C.byref(err))
+            # per-symbol hot path: one outcome and error struct per handle
+            if not payload.is_contiguous():
+                raise ValueError("device buffer must be contiguous")
+            bufs = self.__dict__.get("_push_bufs")
+            if bufs is None:
+                o, e = _Push(), _Error()
+                bufs = self._push_bufs = (o, e, C.byref(o), C.byref(e))
+            o, err = bufs[0], bufs[1]
+            st = self._lib.dec_push_device(self._ptr, index, payload.data_ptr(), payload.nbytes, bufs[2], bufs[3])
         else:
+            err, o = _Error(), _Push()
             p, ln, keep = _host_view(payload)
             st = self._lib.dec_push(self._ptr, index, p, ln, C.byref(o), C.byref(err))
-        self._lib.check(st, err)
+        if st:
+            self._lib.check(st, err)
         kind = PushOutcomeKind(o.kind)
         if kind == PushOutcomeKind.ADVANCED:
             return PushOutcome.advanced(int(o.rank), int(o.received))
