@@ -437,7 +437,9 @@ SCRS_API int32_t scrs_stripe_batch_autotune(scrs_stripe_batch* batch, void* stre
  * load != 0, loads for the current device) ahead of time, so the first
  * batch does not pay the compile; without load it needs no device.
  * SCRS_ERR_BAD_ARGUMENT for an engine or geometry that is not specialised,
- * SCRS_ERR_JIT (a = nvrtcResult) when the compile fails. */
+ * SCRS_ERR_JIT (a = nvrtcResult) when the compile fails or NVRTC cannot be
+ * loaded (it is opened on first use; without it every stripe stays on the
+ * precompiled kernels). */
 SCRS_API int32_t scrs_jit_prepare(int32_t engine, uint32_t k, uint32_t m, int32_t load,
                                   uint64_t* cubin_bytes, scrs_error* err);
 /* Whether scrs_stripe_batch_set specialises eligible encode stripes (1, the

@@ -19,7 +19,6 @@ SOURCES = ["mxk_kernels.cu", "afft.cu", "engines.cu", "batch.cu", "noalloc.cu", 
 GEN = HERE / "_lib" / "gen"
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-gencode", "arch=compute_100a,code=sm_100a",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr", "-I", str(GEN)]
-CUDA_LIB = Path("/usr/local/cuda/lib64")
 # headers the run-time compiler (jit.cu) is given: name as #included -> file
 JIT_HEADERS = [("mxk_spec.cuh", CSRC / "mxk_spec.cuh"), ("mxk_device.cuh", CSRC / "mxk_device.cuh"),
                ("common.cuh", CSRC / "common.cuh"), ("kernels.cuh", CSRC / "kernels.cuh")]
@@ -90,8 +89,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     if failed:
         raise RuntimeError("nvcc compilation failed")
     link = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "static",
-            *[str(o) for o in objs], "-L", str(CUDA_LIB), "-lnvrtc", "-Xlinker", f"-rpath={CUDA_LIB}",
-            "-o", str(OUT)]
+            *[str(o) for o in objs], "-ldl", "-o", str(OUT)]
     subprocess.run(link, check=True)
     return OUT
 

@@ -6,6 +6,7 @@
 // for the life of the process.
 #include "jit.h"
 
+#include <dlfcn.h>
 #include <nvrtc.h>
 
 #include <algorithm>
@@ -104,6 +105,36 @@ void emit_network(std::ostringstream& o, uint8_t c, const char* acc, int& tmp) {
     }
 }
 
+// ---- NVRTC, loaded on first use ----------------------------------------------------
+// The library does not link NVRTC: without it, nothing is specialised and
+// every stripe runs on the precompiled kernels.
+struct Nvrtc {
+    bool ok = false;
+    nvrtcResult (*create)(nvrtcProgram*, const char*, const char*, int, const char* const*, const char* const*);
+    nvrtcResult (*compile)(nvrtcProgram, int, const char* const*);
+    nvrtcResult (*cubin_size)(nvrtcProgram, size_t*);
+    nvrtcResult (*cubin)(nvrtcProgram, char*);
+    nvrtcResult (*destroy)(nvrtcProgram*);
+};
+
+const Nvrtc& nvrtc() {
+    static Nvrtc n = [] {
+        Nvrtc r{};
+        void* h = nullptr;
+        for (const char* name : {"libnvrtc.so.12", "libnvrtc.so", "/usr/local/cuda/lib64/libnvrtc.so.12"})
+            if ((h = dlopen(name, RTLD_NOW | RTLD_LOCAL))) break;
+        if (!h) return r;
+        r.create = reinterpret_cast<decltype(r.create)>(dlsym(h, "nvrtcCreateProgram"));
+        r.compile = reinterpret_cast<decltype(r.compile)>(dlsym(h, "nvrtcCompileProgram"));
+        r.cubin_size = reinterpret_cast<decltype(r.cubin_size)>(dlsym(h, "nvrtcGetCUBINSize"));
+        r.cubin = reinterpret_cast<decltype(r.cubin)>(dlsym(h, "nvrtcGetCUBIN"));
+        r.destroy = reinterpret_cast<decltype(r.destroy)>(dlsym(h, "nvrtcDestroyProgram"));
+        r.ok = r.create && r.compile && r.cubin_size && r.cubin && r.destroy;
+        return r;
+    }();
+    return n;
+}
+
 // ---- compiled kernels ------------------------------------------------------------
 struct Compiled {
     int32_t status = SCRS_OK;  // SCRS_ERR_JIT when the compile failed (detail = nvrtcResult)
@@ -123,21 +154,26 @@ std::map<Key, std::unique_ptr<Compiled>>& cache() {
 }
 
 void compile(Compiled& c, int32_t engine, uint32_t k, uint32_t m) {
+    const Nvrtc& nv = nvrtc();
+    if (!nv.ok) {  // no NVRTC in this process
+        c.status = SCRS_ERR_JIT;
+        c.detail = (uint64_t)NVRTC_ERROR_INTERNAL_ERROR;
+        return;
+    }
     const std::string src = jit_source(engine, k, m);
     nvrtcProgram prog = nullptr;
-    nvrtcResult r = nvrtcCreateProgram(&prog, src.c_str(), "scrs_spec.cu", kJitHeaderCount, kJitHeaderTexts,
-                                       kJitHeaderNames);
+    nvrtcResult r = nv.create(&prog, src.c_str(), "scrs_spec.cu", kJitHeaderCount, kJitHeaderTexts, kJitHeaderNames);
     if (r == NVRTC_SUCCESS) {
         const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17"};
-        r = nvrtcCompileProgram(prog, 2, opts);
+        r = nv.compile(prog, 2, opts);
         size_t n = 0;
-        if (r == NVRTC_SUCCESS) r = nvrtcGetCUBINSize(prog, &n);
+        if (r == NVRTC_SUCCESS) r = nv.cubin_size(prog, &n);
         if (r == NVRTC_SUCCESS) {
             c.cubin.resize(n);
-            r = nvrtcGetCUBIN(prog, c.cubin.data());
+            r = nv.cubin(prog, c.cubin.data());
         }
     }
-    if (prog) nvrtcDestroyProgram(&prog);
+    if (prog) nv.destroy(&prog);
     if (r != NVRTC_SUCCESS) {
         c.status = SCRS_ERR_JIT;
         c.detail = (uint64_t)r;
