@@ -19,7 +19,7 @@
 
 namespace scrs {
 
-extern "C" __global__ void __launch_bounds__(kThreads, 8)
+extern "C" __global__ void __launch_bounds__(kThreads, 10)
     scrs_spec_drain(const MxkTask* __restrict__ tasks, const uint32_t* __restrict__ item_task, uint32_t item_lo,
                     uint32_t total_items, uint32_t* work_counter, int32_t* status) {
     using G = FieldGeom<0>;
