@@ -257,8 +257,15 @@ SCRS_API int32_t scrs_incremental_encoder_profile(const scrs_incremental_encoder
 SCRS_API int32_t scrs_inc_feed(scrs_incremental_encoder* enc, uint64_t index,
                       const uint8_t* data, uint64_t data_len,
                       scrs_error* err);
-/* Device-resident feed: d_data is a device pointer; enqueued on the
- * encoder's own stream (ordered with later calls on this handle). */
+/* Device-resident feed: d_data is a device pointer.  The row is copied on
+ * `stream`, so the copy follows the caller's earlier work on that stream and
+ * the caller may overwrite d_data with work enqueued there afterwards; later
+ * calls on this handle wait for the copy. */
+SCRS_API int32_t scrs_inc_feed_device_stream(scrs_incremental_encoder* enc, uint64_t index,
+                                    const uint8_t* d_data, uint64_t data_len,
+                                    void* stream, scrs_error* err);
+/* scrs_inc_feed_device_stream on the legacy default stream (which orders
+ * the copy with the work of every blocking stream of the context). */
 SCRS_API int32_t scrs_inc_feed_device(scrs_incremental_encoder* enc, uint64_t index,
                              const uint8_t* d_data, uint64_t data_len,
                              scrs_error* err);
@@ -266,7 +273,9 @@ SCRS_API int32_t scrs_inc_feed_device(scrs_incremental_encoder* enc, uint64_t in
  * repair; across the ABI the repair is copied into `dst` (host). */
 SCRS_API int32_t scrs_inc_repair(const scrs_incremental_encoder* enc, uint64_t index,
                         uint8_t* dst, uint64_t dst_len, scrs_error* err);
-/* Borrow form: device address of repair `index` (valid until destroy). */
+/* Borrow form: device address of repair `index`, complete when the call
+ * returns.  The address stays valid until destroy; the bytes there change
+ * with the next reset or fold of new feeds. */
 SCRS_API int32_t scrs_inc_repair_device(const scrs_incremental_encoder* enc,
                                uint64_t index, const uint8_t** d_repair,
                                scrs_error* err);
@@ -286,7 +295,16 @@ SCRS_API void scrs_decode_scratch_destroy(scrs_decode_scratch* scratch);
 SCRS_API int32_t scrs_dec_push(scrs_decoder* dec, uint64_t index,
                       const uint8_t* payload, uint64_t payload_len,
                       scrs_push_outcome* outcome, scrs_error* err);
-/* Device-resident push: d_payload is a device pointer. */
+/* Device-resident push: d_payload is a device pointer, copied on `stream`
+ * into the decoder's payload buffer (after the caller's earlier work on
+ * `stream`; the caller may overwrite d_payload with work enqueued there
+ * afterwards).  The copy also waits for the reads of the last finalize, so
+ * a reset decoder can be refilled while that decode still runs. */
+SCRS_API int32_t scrs_dec_push_device_stream(scrs_decoder* dec, uint64_t index,
+                                    const uint8_t* d_payload, uint64_t payload_len,
+                                    void* stream, scrs_push_outcome* outcome,
+                                    scrs_error* err);
+/* scrs_dec_push_device_stream on the legacy default stream. */
 SCRS_API int32_t scrs_dec_push_device(scrs_decoder* dec, uint64_t index,
                              const uint8_t* d_payload, uint64_t payload_len,
                              scrs_push_outcome* outcome, scrs_error* err);
@@ -302,7 +320,11 @@ SCRS_API int32_t scrs_dec_finalize_into_with(scrs_decoder* dec, uint8_t* out,
                                     uint64_t out_len,
                                     scrs_decode_scratch* scratch,
                                     scrs_error* err);
-/* Device-resident finalize into d_out (device), enqueued on `stream`. */
+/* Device-resident finalize into d_out (device), enqueued on `stream` after
+ * the pushes' copies; returns without waiting.  Later pushes (after a reset)
+ * and host uploads wait on the device for this decode's reads of the
+ * payload buffer; a host push after a reset waits on the host for the
+ * upload of the staged rows. */
 SCRS_API int32_t scrs_dec_finalize_into_with_device(scrs_decoder* dec, uint8_t* d_out,
                                            uint64_t out_len,
                                            scrs_decode_scratch* scratch,

@@ -215,6 +215,7 @@ extern "C" {
     pub fn scrs_incremental_encoder_destroy(enc: *mut scrs_incremental_encoder);
     pub fn scrs_incremental_encoder_profile(enc: *const scrs_incremental_encoder, out: *mut scrs_profile) -> i32;
     pub fn scrs_inc_feed(enc: *mut scrs_incremental_encoder, index: u64, data: *const u8, data_len: u64, err: *mut scrs_error) -> i32;
+    pub fn scrs_inc_feed_device_stream(enc: *mut scrs_incremental_encoder, index: u64, d_data: *const u8, data_len: u64, stream: *mut c_void, err: *mut scrs_error) -> i32;
     pub fn scrs_inc_feed_device(enc: *mut scrs_incremental_encoder, index: u64, d_data: *const u8, data_len: u64, err: *mut scrs_error) -> i32;
     pub fn scrs_inc_repair(enc: *const scrs_incremental_encoder, index: u64, dst: *mut u8, dst_len: u64, err: *mut scrs_error) -> i32;
     pub fn scrs_inc_repair_device(enc: *const scrs_incremental_encoder, index: u64, d_repair: *mut *const u8, err: *mut scrs_error) -> i32;
@@ -226,6 +227,7 @@ extern "C" {
     pub fn scrs_decoder_scratch(dec: *const scrs_decoder, out: *mut *mut scrs_decode_scratch, err: *mut scrs_error) -> i32;
     pub fn scrs_decode_scratch_destroy(scratch: *mut scrs_decode_scratch);
     pub fn scrs_dec_push(dec: *mut scrs_decoder, index: u64, payload: *const u8, payload_len: u64, outcome: *mut scrs_push_outcome, err: *mut scrs_error) -> i32;
+    pub fn scrs_dec_push_device_stream(dec: *mut scrs_decoder, index: u64, d_payload: *const u8, payload_len: u64, stream: *mut c_void, outcome: *mut scrs_push_outcome, err: *mut scrs_error) -> i32;
     pub fn scrs_dec_push_device(dec: *mut scrs_decoder, index: u64, d_payload: *const u8, payload_len: u64, outcome: *mut scrs_push_outcome, err: *mut scrs_error) -> i32;
     pub fn scrs_dec_is_complete(dec: *const scrs_decoder) -> i32;
     pub fn scrs_dec_rank(dec: *const scrs_decoder) -> u64;

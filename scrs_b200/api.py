@@ -203,8 +203,10 @@ _DEVICE_SIGNATURES = [
     ("batch_decode_into_with_device", _I32, [_P, C.POINTER(C.c_uint64), _BUF, _U64, _BUF, _U64, _P, _P,
                                              C.POINTER(_Error)]),
     ("inc_feed_device", _I32, [_P, _U64, _BUF, _U64, C.POINTER(_Error)]),
+    ("inc_feed_device_stream", _I32, [_P, _U64, _BUF, _U64, _P, C.POINTER(_Error)]),
     ("inc_repair_device", _I32, [_P, _U64, C.POINTER(C.c_void_p), C.POINTER(_Error)]),
     ("dec_push_device", _I32, [_P, _U64, _BUF, _U64, C.POINTER(_Push), C.POINTER(_Error)]),
+    ("dec_push_device_stream", _I32, [_P, _U64, _BUF, _U64, _P, C.POINTER(_Push), C.POINTER(_Error)]),
     ("dec_finalize_into_with_device", _I32, [_P, _BUF, _U64, _P, _P, C.POINTER(_Error)]),
     ("status_name", C.c_char_p, [_I32]),
     ("batch_decode_scratch_recipe_hits", _U64, [_P]),
@@ -270,6 +272,21 @@ def _device_view(x) -> Tuple[int, int]:
     if not x.is_contiguous():
         raise ValueError("device buffer must be contiguous")
     return x.data_ptr(), x.numel() * x.element_size()
+
+
+_raw_stream = None
+
+
+def _tensor_stream(t) -> int:
+    """Raw handle of the current CUDA stream of tensor t's device (the stream
+    torch orders t's producers on)."""
+    global _raw_stream
+    if _raw_stream is None:
+        import torch
+
+        get = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+        _raw_stream = get if get is not None else (lambda dev: torch.cuda.current_stream(dev).cuda_stream)
+    return _raw_stream(t.get_device())
 
 
 def _stream_ptr(stream) -> int:
@@ -482,7 +499,9 @@ class IncrementalEncoder(_Handle):
 
     _destroy = "incremental_encoder_destroy"
 
-    def feed(self, index: int, data):
+    def feed(self, index: int, data, stream=None):
+        """Feed data symbol `index`.  A CUDA tensor is copied on `stream`
+        (default: the current stream of its device)."""
         if _is_cuda_tensor(data):
             # per-symbol hot path: one error struct per handle, no temporaries
             if data.is_contiguous():
@@ -490,7 +509,8 @@ class IncrementalEncoder(_Handle):
                 if errs is None:
                     e = _Error()
                     errs = self._errs = (e, C.byref(e))
-                st = self._lib.inc_feed_device(self._ptr, index, data.data_ptr(), data.nbytes, errs[1])
+                sp = _tensor_stream(data) if stream is None else _stream_ptr(stream)
+                st = self._lib.inc_feed_device_stream(self._ptr, index, data.data_ptr(), data.nbytes, sp, errs[1])
                 if st:
                     self._lib.check(st, errs[0])
                 return
@@ -527,7 +547,9 @@ class Decoder(_Handle):
         self._lib.check(self._lib.decoder_scratch(self._ptr, C.byref(out), C.byref(err)), err)
         return DecodeScratch(self._lib, out, self.profile)
 
-    def push(self, index: int, payload) -> PushOutcome:
+    def push(self, index: int, payload, stream=None) -> PushOutcome:
+        """Push symbol `index`.  A CUDA tensor is copied on `stream` (default:
+        the current stream of its device)."""
         if _is_cuda_tensor(payload):
             # per-symbol hot path: one outcome and error struct per handle
             if not payload.is_contiguous():
@@ -537,7 +559,9 @@ class Decoder(_Handle):
                 o, e = _Push(), _Error()
                 bufs = self._push_bufs = (o, e, C.byref(o), C.byref(e))
             o, err = bufs[0], bufs[1]
-            st = self._lib.dec_push_device(self._ptr, index, payload.data_ptr(), payload.nbytes, bufs[2], bufs[3])
+            sp = _tensor_stream(payload) if stream is None else _stream_ptr(stream)
+            st = self._lib.dec_push_device_stream(self._ptr, index, payload.data_ptr(), payload.nbytes, sp, bufs[2],
+                                                  bufs[3])
         else:
             err, o = _Error(), _Push()
             p, ln, keep = _host_view(payload)

@@ -447,9 +447,19 @@ struct scrs_decoder {
     uint64_t distinct = 0, received = 0;
     TowerTables tower;
     std::unique_ptr<AfftCodec> afft;
-    cudaEvent_t uploaded = nullptr;  // orders the payload uploads before a caller's stream
+    // Stream order around the payload buffer.  Device pushes copy on the
+    // caller's stream, chained on one stream at a time (push_stream; `pushed`
+    // is recorded there when the chain moves or a finalize starts); a
+    // finalize records `consumed` on its stream after the work that reads the
+    // payloads, and the next writer of a payload row waits on it; host-staged
+    // rows go up on the decoder's own stream (`uploaded`).
+    cudaEvent_t uploaded = nullptr, pushed = nullptr, consumed = nullptr;
+    cudaStream_t push_stream = nullptr, consumed_waited = nullptr;
+    bool push_pending = false, consumed_pending = false, upload_inflight = false;
     ~scrs_decoder() {
         if (uploaded) cudaEventDestroy(uploaded);
+        if (pushed) cudaEventDestroy(pushed);
+        if (consumed) cudaEventDestroy(consumed);
     }
 };
 
@@ -474,6 +484,8 @@ extern "C" int32_t scrs_decoder_create(const scrs_profile* p, scrs_decoder** out
     SCRS_CUDA(d->stream.init());
     SCRS_CUDA(d->status.init());
     SCRS_CUDA(cudaEventCreateWithFlags(&d->uploaded, cudaEventDisableTiming));
+    SCRS_CUDA(cudaEventCreateWithFlags(&d->pushed, cudaEventDisableTiming));
+    SCRS_CUDA(cudaEventCreateWithFlags(&d->consumed, cudaEventDisableTiming));
     SCRS_CUDA(d->payloads.ensure(n * L));
     SCRS_CUDA(d->staging.ensure(n * L));
     d->have.assign(n, 0);
@@ -531,7 +543,7 @@ namespace {
 
 // symbol_sink.rs:36-54 with the checks of decoder/streaming.rs:388-429.
 int32_t push_common(scrs_decoder* d, uint64_t idx, const uint8_t* payload, uint64_t len, bool device,
-                    scrs_push_outcome* outcome, scrs_error* err) {
+                    cudaStream_t cs, scrs_push_outcome* outcome, scrs_error* err) {
     if (!d) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
     const uint64_t n = d->p.k + d->p.m, L = d->p.symbol_len;
     if (idx >= n) return set_err(err, SCRS_DECODE_INDEX_OUT_OF_RANGE, idx, n);
@@ -544,10 +556,27 @@ int32_t push_common(scrs_decoder* d, uint64_t idx, const uint8_t* payload, uint6
         o.kind = SCRS_PUSH_DEPENDENT;
     } else {
         if (device) {
-            SCRS_CUDA(cudaMemcpyAsync(d->payloads.as<uint8_t>() + idx * L, payload, L, cudaMemcpyDeviceToDevice,
-                                      d->stream.s));
+            // after the last finalize's reads of the payload rows
+            if (d->consumed_pending && d->consumed_waited != cs) {
+                SCRS_CUDA(cudaStreamWaitEvent(cs, d->consumed, 0));
+                d->consumed_waited = cs;
+            }
+            // the copies are chained on one stream at a time: moving to
+            // another, it waits for the earlier stream's copies (so a row
+            // pushed again after a reset lands last)
+            if (d->push_pending && d->push_stream != cs) {
+                SCRS_CUDA(cudaEventRecord(d->pushed, d->push_stream));
+                SCRS_CUDA(cudaStreamWaitEvent(cs, d->pushed, 0));
+            }
+            SCRS_CUDA(cudaMemcpyAsync(d->payloads.as<uint8_t>() + idx * L, payload, L, cudaMemcpyDeviceToDevice, cs));
+            d->push_stream = cs;
+            d->push_pending = true;
             d->on_host[idx] = 0;
         } else {
+            if (d->upload_inflight) {  // the staging rows of an earlier finalize may still be going up
+                SCRS_CUDA(cudaStreamSynchronize(d->stream.s));
+                d->upload_inflight = false;
+            }
             memcpy(d->staging.as<uint8_t>() + idx * L, payload, L);
             d->on_host[idx] = 1;
         }
@@ -568,6 +597,7 @@ int32_t push_common(scrs_decoder* d, uint64_t idx, const uint8_t* payload, uint6
 // Upload host-staged payload rows in contiguous runs.
 int32_t upload_staged(scrs_decoder* d, scrs_error* err) {
     const uint64_t n = d->p.k + d->p.m, L = d->p.symbol_len;
+    bool waited = false;
     uint64_t i = 0;
     while (i < n) {
         if (!(d->have[i] && d->on_host[i])) {
@@ -576,24 +606,52 @@ int32_t upload_staged(scrs_decoder* d, scrs_error* err) {
         }
         uint64_t j = i;
         while (j < n && d->have[j] && d->on_host[j]) j++;
+        if (!waited && d->consumed_pending && d->consumed_waited != d->stream.s) {
+            SCRS_CUDA(cudaStreamWaitEvent(d->stream.s, d->consumed, 0));  // after the last finalize's reads
+            waited = true;
+        }
         SCRS_CUDA(cudaMemcpyAsync(d->payloads.as<uint8_t>() + i * L, d->staging.as<uint8_t>() + i * L, (j - i) * L,
                                   cudaMemcpyHostToDevice, d->stream.s));
         for (uint64_t t = i; t < j; t++) d->on_host[t] = 0;
+        d->upload_inflight = true;
         i = j;
     }
     return SCRS_OK;
 }
 
+int32_t finalize_enqueue(scrs_decoder* d, uint8_t* d_out, scrs_decode_scratch* s, cudaStream_t st,
+                         scrs_error* err);
+
 int32_t finalize_device(scrs_decoder* d, uint8_t* d_out, scrs_decode_scratch* s, cudaStream_t st,
                         scrs_error* err) {
-    const uint32_t k = (uint32_t)d->p.k, m = (uint32_t)d->p.m;
-    const uint64_t L = d->p.symbol_len;
     int32_t r = upload_staged(d, err);
     if (r) return r;
     if (st != d->stream.s) {  // order the payload uploads before the caller's stream
         SCRS_CUDA(cudaEventRecord(d->uploaded, d->stream.s));
         SCRS_CUDA(cudaStreamWaitEvent(st, d->uploaded, 0));
     }
+    if (d->push_pending) {  // and the device pushes' copies
+        if (d->push_stream != st) {
+            SCRS_CUDA(cudaEventRecord(d->pushed, d->push_stream));
+            SCRS_CUDA(cudaStreamWaitEvent(st, d->pushed, 0));
+        }
+        d->push_pending = false;
+    }
+    // an earlier finalize's reads on another stream: keep `consumed` covering them
+    if (d->consumed_pending && d->consumed_waited != st) SCRS_CUDA(cudaStreamWaitEvent(st, d->consumed, 0));
+    r = finalize_enqueue(d, d_out, s, st, err);
+    if (r) return r;
+    SCRS_CUDA(cudaEventRecord(d->consumed, st));  // the next writer of a payload row waits on this
+    d->consumed_pending = true;
+    d->consumed_waited = st;
+    return SCRS_OK;
+}
+
+// The decode itself, enqueued on st once the payload rows are in place.
+int32_t finalize_enqueue(scrs_decoder* d, uint8_t* d_out, scrs_decode_scratch* s, cudaStream_t st,
+                         scrs_error* err) {
+    const uint32_t k = (uint32_t)d->p.k, m = (uint32_t)d->p.m;
+    const uint64_t L = d->p.symbol_len;
     if (d->afft) return d->afft->decode(d->payloads.as<uint8_t>(), d->have.data(), d_out, *s->afft,
                                         d->status.dev, st, err);
     // build_recipe (decoder/streaming.rs:163-194, tower/decoder.rs:218-247)
@@ -637,6 +695,7 @@ int32_t finalize_host(scrs_decoder* d, uint8_t* out, uint64_t out_len, scrs_deco
     if (r) return r;
     SCRS_CUDA(cudaMemcpyAsync(out, d_out, out_len, cudaMemcpyDeviceToHost, d->stream.s));
     SCRS_CUDA(cudaStreamSynchronize(d->stream.s));
+    d->consumed_pending = d->upload_inflight = false;
     r = take_status(d->status, err);
     if (r) return r;
     return set_err(err, SCRS_OK);
@@ -646,12 +705,17 @@ int32_t finalize_host(scrs_decoder* d, uint8_t* out, uint64_t out_len, scrs_deco
 
 extern "C" int32_t scrs_dec_push(scrs_decoder* d, uint64_t idx, const uint8_t* payload, uint64_t len,
                                  scrs_push_outcome* outcome, scrs_error* err) {
-    return push_common(d, idx, payload, len, false, outcome, err);
+    return push_common(d, idx, payload, len, false, nullptr, outcome, err);
 }
 
 extern "C" int32_t scrs_dec_push_device(scrs_decoder* d, uint64_t idx, const uint8_t* payload, uint64_t len,
                                         scrs_push_outcome* outcome, scrs_error* err) {
-    return push_common(d, idx, payload, len, true, outcome, err);
+    return push_common(d, idx, payload, len, true, cudaStreamLegacy, outcome, err);
+}
+
+extern "C" int32_t scrs_dec_push_device_stream(scrs_decoder* d, uint64_t idx, const uint8_t* payload, uint64_t len,
+                                               void* stream, scrs_push_outcome* outcome, scrs_error* err) {
+    return push_common(d, idx, payload, len, true, (cudaStream_t)stream, outcome, err);
 }
 
 extern "C" int32_t scrs_dec_is_complete(const scrs_decoder* d) { return d && d->distinct >= d->p.k; }
@@ -944,6 +1008,15 @@ struct scrs_incremental_encoder {
     std::vector<uint8_t> fed, pending_host, pending_dev;
     std::vector<uint16_t> pending;
     uint64_t fed_count = 0;
+    // Device feeds copy on the caller's stream, chained on one stream at a
+    // time (copy_stream); `copied` is recorded there when the chain moves or
+    // a fold starts, and the fold waits on it.
+    cudaEvent_t copied = nullptr;
+    cudaStream_t copy_stream = nullptr;
+    bool copy_pending = false;
+    ~scrs_incremental_encoder() {
+        if (copied) cudaEventDestroy(copied);
+    }
 };
 
 extern "C" int32_t scrs_incremental_encoder_create(const scrs_profile* p, scrs_incremental_encoder** out,
@@ -959,6 +1032,7 @@ extern "C" int32_t scrs_incremental_encoder_create(const scrs_profile* p, scrs_i
     const uint64_t k = p->k, m = p->m, L = p->symbol_len;
     SCRS_CUDA(e->stream.init());
     SCRS_CUDA(e->status.init());
+    SCRS_CUDA(cudaEventCreateWithFlags(&e->copied, cudaEventDisableTiming));
     if (p->engine == SCRS_ENGINE_TOWER) {
         std::vector<uint16_t> pw(k + m), c(k * m);
         hf::tower_powers((uint32_t)(k + m), pw.data());
@@ -995,7 +1069,7 @@ extern "C" int32_t scrs_incremental_encoder_profile(const scrs_incremental_encod
 namespace {
 
 int32_t feed_common(scrs_incremental_encoder* e, uint64_t idx, const uint8_t* data, uint64_t len, bool device,
-                    scrs_error* err) {
+                    cudaStream_t cs, scrs_error* err) {
     if (!e) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
     const uint64_t k = e->p.k, m = e->p.m, L = e->p.symbol_len;
     // encoder/streaming.rs:163-177, tower/encoder.rs:90-104
@@ -1004,7 +1078,15 @@ int32_t feed_common(scrs_incremental_encoder* e, uint64_t idx, const uint8_t* da
     if (e->fed[idx]) return set_err(err, SCRS_ENCODE_DUPLICATE_DATA, idx);
     if (!data) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
     if (device) {
-        SCRS_CUDA(cudaMemcpyAsync(e->data.as<uint8_t>() + idx * L, data, L, cudaMemcpyDeviceToDevice, e->stream.s));
+        // rows are written again only after a reset, which waits for the folds
+        // that read them; chain this stream after an earlier one's copies
+        if (e->copy_pending && e->copy_stream != cs) {
+            SCRS_CUDA(cudaEventRecord(e->copied, e->copy_stream));
+            SCRS_CUDA(cudaStreamWaitEvent(cs, e->copied, 0));
+        }
+        SCRS_CUDA(cudaMemcpyAsync(e->data.as<uint8_t>() + idx * L, data, L, cudaMemcpyDeviceToDevice, cs));
+        e->copy_stream = cs;
+        e->copy_pending = true;
         e->pending_dev[idx] = 1;
     } else {
         memcpy(e->staging.as<uint8_t>() + idx * L, data, L);
@@ -1033,6 +1115,11 @@ int32_t flush(scrs_incremental_encoder* e, scrs_error* err) {
         SCRS_CUDA(cudaMemcpyAsync(e->data.as<uint8_t>() + i * L, e->staging.as<uint8_t>() + i * L, (j - i) * L,
                                   cudaMemcpyHostToDevice, st));
         i = j;
+    }
+    if (e->copy_pending) {  // the device feeds' copies
+        SCRS_CUDA(cudaEventRecord(e->copied, e->copy_stream));
+        SCRS_CUDA(cudaStreamWaitEvent(st, e->copied, 0));
+        e->copy_pending = false;
     }
     std::sort(e->pending.begin(), e->pending.end());
     SCRS_CUDA(cudaMemcpyAsync(e->rows.p, e->pending.data(), e->pending.size() * 2, cudaMemcpyHostToDevice, st));
@@ -1064,12 +1151,17 @@ int32_t flush(scrs_incremental_encoder* e, scrs_error* err) {
 
 extern "C" int32_t scrs_inc_feed(scrs_incremental_encoder* e, uint64_t idx, const uint8_t* data, uint64_t len,
                                  scrs_error* err) {
-    return feed_common(e, idx, data, len, false, err);
+    return feed_common(e, idx, data, len, false, nullptr, err);
 }
 
 extern "C" int32_t scrs_inc_feed_device(scrs_incremental_encoder* e, uint64_t idx, const uint8_t* data,
                                         uint64_t len, scrs_error* err) {
-    return feed_common(e, idx, data, len, true, err);
+    return feed_common(e, idx, data, len, true, cudaStreamLegacy, err);
+}
+
+extern "C" int32_t scrs_inc_feed_device_stream(scrs_incremental_encoder* e, uint64_t idx, const uint8_t* data,
+                                               uint64_t len, void* stream, scrs_error* err) {
+    return feed_common(e, idx, data, len, true, (cudaStream_t)stream, err);
 }
 
 // encoder/streaming.rs:197-206, tower/encoder.rs:122-131
