@@ -499,6 +499,9 @@ typedef struct scrs_request {
     uint8_t* out;        /* device: encode m*L repairs; decode k*L data        */
     const uint64_t* indices; /* host, decode only: k indices (copied at submit) */
     uint64_t tag;        /* returned with the completion                       */
+    void* stream;        /* the stream `in` was written on (NULL: the legacy
+                            default stream): the request's device work waits
+                            for the work enqueued there before the submit      */
 } scrs_request;
 typedef struct scrs_completion {
     uint64_t ticket, tag;
@@ -517,7 +520,9 @@ SCRS_API int32_t scrs_server_create(uint64_t memory_budget, uint32_t slots,
 SCRS_API void scrs_server_destroy(scrs_server* server);
 /* Validates (profile, decode indices, budget: SCRS_ERR_CAPACITY when the
  * request alone exceeds it), queues, and admits what fits.  Buffers must
- * stay valid until the request's completion is returned. */
+ * stay valid until the request's completion is returned; `out` is complete
+ * on the device when it is.  The input is read after the work enqueued on
+ * req->stream before this call. */
 SCRS_API int32_t scrs_server_submit(scrs_server* server, const scrs_request* req,
                                     uint64_t* ticket, scrs_error* err);
 /* Non-blocking: retires finished slots, admits waiting requests and returns

@@ -160,6 +160,7 @@ pub struct scrs_request {
     pub out: *mut u8,
     pub indices: *const u64,
     pub tag: u64,
+    pub stream: *mut c_void,
 }
 
 #[repr(C)]

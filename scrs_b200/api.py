@@ -290,10 +290,15 @@ def _tensor_stream(t) -> int:
 
 
 def _stream_ptr(stream) -> int:
+    """Raw handle of `stream` (a torch stream or an int); None: torch's current
+    stream of the current device (0, the legacy default stream, without torch)."""
     if stream is None:
         try:
             import torch
 
+            get = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+            if get is not None:
+                return get(torch.cuda.current_device())
             return torch.cuda.current_stream().cuda_stream
         except Exception:  # pragma: no cover
             return 0

@@ -73,6 +73,7 @@ uint64_t resident_estimate(const scrs_profile& p, int32_t op) {
 
 struct Req {
     scrs_request d{};
+    cudaEvent_t ready = nullptr;  // recorded on the caller's stream at submit
     uint64_t ticket = 0;
     uint64_t t_submit = 0;
     uint64_t bytes = 0;  // input + output
@@ -92,6 +93,7 @@ struct Slot {
     bool used_batch = false;
     int32_t launch_code = 0;
     scrs_error launch_err{};
+    std::vector<void*> seen_streams;  // scratch of admit()
     uint64_t held = 0;  // request bytes held while running
     bool busy = false;
     ~Slot() {
@@ -114,7 +116,14 @@ struct scrs_server {
     std::vector<std::unique_ptr<Slot>> slots;
     std::deque<Req> queue;
     std::vector<scrs_completion> ready;  // finished but not yet returned
+    std::vector<cudaEvent_t> free_events;  // input-ready events for reuse
     scrs_server_stats stats{};
+    ~scrs_server() {
+        for (cudaEvent_t e : free_events) cudaEventDestroy(e);
+        for (const Req& r : queue) cudaEventDestroy(r.ready);
+        for (auto& sl : slots)
+            for (const Req& r : sl->running) cudaEventDestroy(r.ready);
+    }
 };
 
 namespace {
@@ -263,7 +272,10 @@ void retire(scrs_server* s, Slot& sl, uint64_t t_done) {
         if (!status && R->dec) status = internal_batch_decoder_status(R->dec, &e);
     }
     if (!status) status = take_status(sl.status, &e);
-    for (const Req& r : sl.running) finish(s, r, status, t_done);
+    for (const Req& r : sl.running) {
+        finish(s, r, status, t_done);
+        s->free_events.push_back(r.ready);  // its wait has run: reusable
+    }
     s->in_use -= sl.held;
     sl.held = 0;
     sl.running.clear();
@@ -271,6 +283,22 @@ void retire(scrs_server* s, Slot& sl, uint64_t t_done) {
     sl.used_batch = false;
     sl.launch_code = 0;
     sl.busy = false;
+}
+
+// Make the slot's stream wait for the work that wrote its requests' inputs:
+// one wait per distinct caller stream, on the event of that stream's latest
+// request (events recorded later on a stream cover the earlier ones).
+int32_t wait_inputs(Slot& sl) {
+    std::vector<void*>& seen = sl.seen_streams;
+    seen.clear();
+    for (size_t q = sl.running.size(); q-- > 0;) {
+        const Req& r = sl.running[q];
+        if (std::find(seen.begin(), seen.end(), r.d.stream) != seen.end()) continue;
+        seen.push_back(r.d.stream);
+        const cudaError_t e = cudaStreamWaitEvent(sl.stream.s, r.ready, 0);
+        if (e != cudaSuccess) return set_err(&sl.launch_err, SCRS_ERR_CUDA, (uint64_t)e, (uint64_t)__LINE__);
+    }
+    return SCRS_OK;
 }
 
 // Admit waiting requests into idle slots (first come, first served).  A tower
@@ -318,11 +346,13 @@ void admit(scrs_server* s) {
         sl.held = held;
         sl.busy = true;
         sl.running = std::move(group);
-        int32_t rc;
-        if (gf256) {
+        // the inputs' producers first: one wait per distinct caller stream
+        // (the latest request of a stream covers the earlier ones)
+        int32_t rc = wait_inputs(sl);
+        if (!rc && gf256) {
             rc = launch_group(sl, sl.running, &sl.launch_err);
             s->stats.batches++;
-        } else {
+        } else if (!rc) {
             rc = launch_single(s, sl, sl.running[0], &sl.launch_err);
         }
         s->stats.admitted += sl.running.size();
@@ -387,6 +417,15 @@ extern "C" int32_t scrs_server_submit(scrs_server* s, const scrs_request* rq, ui
     r.bytes = k * L + (rq->op == SCRS_OP_ENCODE ? m : k) * L;
     const uint64_t need = r.bytes + (is_gf256(p.engine) ? 0 : resident_estimate(p, rq->op));
     if (need > s->budget) return set_err(err, SCRS_ERR_CAPACITY, need, s->budget);
+    if (s->free_events.empty()) {
+        cudaEvent_t e = nullptr;
+        SCRS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        s->free_events.push_back(e);
+    }
+    r.d.stream = rq->stream ? rq->stream : (void*)cudaStreamLegacy;
+    SCRS_CUDA(cudaEventRecord(s->free_events.back(), (cudaStream_t)r.d.stream));
+    r.ready = s->free_events.back();
+    s->free_events.pop_back();
     r.ticket = s->next_ticket++;
     r.t_submit = now_ns();
     if (ticket) *ticket = r.ticket;

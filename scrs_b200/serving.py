@@ -11,7 +11,7 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
-from .api import Library, _Error, make_error
+from .api import Library, _Error, _stream_ptr, make_error
 
 OP_ENCODE = 0
 OP_DECODE = 1
@@ -20,7 +20,7 @@ OP_DECODE = 1
 class _Request(C.Structure):
     _fields_ = [("op", C.c_int32), ("engine", C.c_int32), ("k", C.c_uint64), ("m", C.c_uint64),
                 ("symbol_len", C.c_uint64), ("in_", C.c_void_p), ("out", C.c_void_p),
-                ("indices", C.POINTER(C.c_uint64)), ("tag", C.c_uint64)]
+                ("indices", C.POINTER(C.c_uint64)), ("tag", C.c_uint64), ("stream", C.c_void_p)]
 
 
 class _Completion(C.Structure):
@@ -90,8 +90,10 @@ class Server:
         self.close()
 
     def submit(self, op: int, engine, k: int, m: int, symbol_len: int, in_ptr: int, out_ptr: int,
-               indices: Optional[Sequence[int]] = None, tag: int = 0) -> int:
-        r = _Request(op, int(engine), k, m, symbol_len, in_ptr, out_ptr, None, tag)
+               indices: Optional[Sequence[int]] = None, tag: int = 0, stream=None) -> int:
+        """Queue one request.  The input is read after the work enqueued
+        before this call on `stream` (default: torch's current stream)."""
+        r = _Request(op, int(engine), k, m, symbol_len, in_ptr, out_ptr, None, tag, _stream_ptr(stream))
         if indices is not None:
             # one conversion for the whole list (a uint64 array passes through
             # as is); the server copies the indices before returning

@@ -108,3 +108,33 @@ def test_submit_errors(gpu):
         srv.submit(OP_DECODE, Engine.GOOD_CAUCHY, 3, 2, 64, p, p, [0, 1, 9])
     assert srv.pending == 0
     srv.close()
+
+
+def test_inputs_written_on_held_back_streams(gpu, oracle):
+    """Inputs produced on side streams that are held back (torch.cuda._sleep)
+    and submitted at once with those streams: every request's work must wait
+    for its producer, including requests coalesced into one GF(256) batch from
+    different streams."""
+    torch = pytest.importorskip("torch")
+    from scrs_b200.serving import Server
+
+    reqs = make_requests(torch, oracle, seed=17)
+    streams = [torch.cuda.Stream() for _ in range(3)]
+    staged = [torch.zeros_like(r[5]) for r in reqs]
+    outs = [torch.full((len(r[-1]),), 0xAB, dtype=torch.uint8, device="cuda") for r in reqs]
+    torch.cuda.synchronize()
+    srv = Server(gpu.lib, 1 << 30, slots=4)
+    for st in streams:
+        with torch.cuda.stream(st):
+            torch.cuda._sleep(40_000_000)  # about 20 ms
+    for q, (op, engine, k, m, L, d_in, idx, exp) in enumerate(reqs):
+        st = streams[q % len(streams)]
+        with torch.cuda.stream(st):
+            staged[q].copy_(d_in)  # lands after the hold
+        srv.submit(op, engine, k, m, L, staged[q].data_ptr(), outs[q].data_ptr(), idx, tag=q, stream=st)
+    done = srv.drain()
+    assert all(c.status == 0 for c in done), [c.status for c in done]
+    torch.cuda.synchronize()
+    for q, r in enumerate(reqs):
+        assert np.array_equal(outs[q].cpu().numpy(), r[-1]), q
+    srv.close()
