@@ -51,8 +51,8 @@ cudaError_t log16_tables(const uint16_t** d_log, const uint16_t** d_exp) {
         Log16Tables* t = new (std::nothrow) Log16Tables();
         if (!t) return cudaErrorMemoryAllocation;
         if ((e = t->log.ensure(65536 * 2)) != cudaSuccess || (e = t->exp.ensure(65535 * 2)) != cudaSuccess ||
-            (e = cudaMemcpy(t->log.p, lg.data(), 65536 * 2, cudaMemcpyHostToDevice)) != cudaSuccess ||
-            (e = cudaMemcpy(t->exp.p, ex.data(), 65535 * 2, cudaMemcpyHostToDevice)) != cudaSuccess) {
+            (e = upload_now(t->log.p, lg.data(), 65536 * 2)) != cudaSuccess ||
+            (e = upload_now(t->exp.p, ex.data(), 65535 * 2)) != cudaSuccess) {
             delete t;
             return e;
         }
@@ -440,15 +440,11 @@ int grid_for(uint64_t items, int threads) {
 // 2^D rows; 2 and 3: the halves below it, each of 2^D rows, D one less).
 cudaError_t run_transform(uint8_t* work, uint32_t G, int D, const uint16_t* factors, bool forward,
                           cudaStream_t st, uint32_t root = 1) {
-    static uint64_t attr = 0;
-    if (first_on_device(attr)) {
-        cudaError_t e = cudaFuncSetAttribute(afft_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             kTileBytes);
-        if (e != cudaSuccess) {
-            attr = 0;
-            return e;
-        }
-    }
+    static std::atomic<uint64_t> attr{0};
+    cudaError_t ea = once_per_device(attr, [] {
+        return cudaFuncSetAttribute(afft_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileBytes);
+    });
+    if (ea != cudaSuccess) return ea;
     // Column groups per tile: up to 8 of one row pair, so that the lanes of a
     // warp (consecutive groups of a few pairs) mostly share the butterfly
     // factor, and tiles stay small enough for two-level-count passes
@@ -492,15 +488,11 @@ uint32_t mod_pow(uint32_t base, uint32_t e) {
 }
 
 cudaError_t run_wht(uint32_t* v, uint32_t ts, int D, cudaStream_t st) {
-    static uint64_t attr = 0;
-    if (first_on_device(attr)) {
-        cudaError_t e = cudaFuncSetAttribute(wht_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             8192 * 4);
-        if (e != cudaSuccess) {
-            attr = 0;
-            return e;
-        }
-    }
+    static std::atomic<uint64_t> attr{0};
+    cudaError_t ea = once_per_device(attr, [] {
+        return cudaFuncSetAttribute(wht_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 4);
+    });
+    if (ea != cudaSuccess) return ea;
     // passes of at most 8 index bits: enough groups per pass to spread over
     // the SMs (one CTA per group of 2^nb elements)
     std::vector<std::pair<int, int>> passes;
@@ -530,16 +522,11 @@ int32_t afft_locator_device(const uint8_t* d_known, uint32_t ts, uint32_t* wa, u
     int D = 0;
     while ((1u << D) < ts) D++;
     if (ts <= kLocatorOneCtaTs) {
-        static uint64_t attr = 0;
-        const int smem = (int)(2 * kLocatorOneCtaTs * sizeof(uint32_t));
-        if (first_on_device(attr)) {
-            cudaError_t e = cudaFuncSetAttribute(locator_one_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 smem);
-            if (e != cudaSuccess) {
-                attr = 0;
-                SCRS_CUDA(e);
-            }
-        }
+        static std::atomic<uint64_t> attr{0};
+        SCRS_CUDA(once_per_device(attr, [] {
+            return cudaFuncSetAttribute(locator_one_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(2 * kLocatorOneCtaTs * sizeof(uint32_t)));
+        }));
         locator_one_cta_kernel<<<1, 1024, 2 * ts * sizeof(uint32_t), st>>>(d_known, ts, mod_pow(32768, (uint32_t)D),
                                                                            lg, ex, values, derivs);
         SCRS_CUDA(cudaGetLastError());
@@ -697,11 +684,11 @@ int32_t AfftWorkspace::init_encode(const AfftCodec& c, scrs_error* err) {
     SCRS_CUDA(known.ensure(c.ts));
     std::vector<uint8_t> hk(c.ts, 0);
     std::fill(hk.begin(), hk.begin() + c.k, 1);
-    SCRS_CUDA(cudaMemcpy(known.p, hk.data(), c.ts, cudaMemcpyHostToDevice));
+    SCRS_CUDA(upload_now(known.p, hk.data(), c.ts));
     std::vector<uint16_t> host_rows(2 * c.m);
     for (uint64_t t = 0; t < c.m; t++) host_rows[t] = (uint16_t)(c.k + t), host_rows[c.m + t] = (uint16_t)t;
     SCRS_CUDA(rows.ensure(host_rows.size() * 2));
-    SCRS_CUDA(cudaMemcpy(rows.p, host_rows.data(), host_rows.size() * 2, cudaMemcpyHostToDevice));
+    SCRS_CUDA(upload_now(rows.p, host_rows.data(), host_rows.size() * 2));
     return SCRS_OK;
 }
 

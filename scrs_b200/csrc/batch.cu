@@ -75,7 +75,12 @@ struct scrs_stripe_batch {
     std::vector<Piece> pieces;
     cudaStream_t s_in = nullptr, s_out = nullptr;
     std::vector<cudaEvent_t> events;  // start, end, then per piece: copied in, computed
+    // recorded on a run's stream after its work: the next set waits for it
+    // before it rewrites the device descriptors and staging that run reads
+    cudaEvent_t ran = nullptr;
+    bool ran_pending = false;
     ~scrs_stripe_batch() {
+        if (ran) cudaEventDestroy(ran);
         if (graph) cudaGraphExecDestroy(graph);
         for (cudaEvent_t e : events) cudaEventDestroy(e);
         if (s_in) cudaStreamDestroy(s_in);
@@ -104,6 +109,7 @@ extern "C" int32_t scrs_stripe_batch_create(uint64_t max_stripes, uint64_t max_i
     SCRS_CUDA(cudaGetDevice(&dev));
     SCRS_CUDA(cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, dev));
     SCRS_CUDA(b->status.init());
+    SCRS_CUDA(cudaEventCreateWithFlags(&b->ran, cudaEventDisableTiming));
     SCRS_CUDA(b->d_tasks.ensure(max_stripes * sizeof(MxkTask)));
     SCRS_CUDA(b->d_plans.ensure(max_stripes * sizeof(CauchyPlanTask)));
     SCRS_CUDA(b->d_counter.ensure(kMaxPieces * sizeof(uint32_t)));
@@ -133,10 +139,35 @@ extern "C" int32_t scrs_stripe_batch_set(scrs_stripe_batch* b, const scrs_stripe
     return stripe_batch_set_impl(b, descs, count, false, nullptr, err);
 }
 
+namespace {
+
+// Wait (on the host, or on `stream` for the staged form) for the last run's
+// reads of the device descriptors and staging before they are rewritten.
+int32_t wait_last_run(scrs_stripe_batch* b, bool async_stream, cudaStream_t stream, scrs_error* err) {
+    if (!b->ran_pending) return SCRS_OK;
+    if (async_stream)
+        SCRS_CUDA(cudaStreamWaitEvent(stream, b->ran, 0));
+    else
+        SCRS_CUDA(cudaEventSynchronize(b->ran));
+    b->ran_pending = false;
+    return SCRS_OK;
+}
+
+// The end of a run on `st`: record it for the next set.
+int32_t ran_on(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
+    SCRS_CUDA(cudaEventRecord(b->ran, st));
+    b->ran_pending = true;
+    return set_err(err, SCRS_OK);
+}
+
+}  // namespace
+
 int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc* descs, uint64_t count,
                                     bool async_stream, cudaStream_t stream, scrs_error* err) {
     if (!b || (count && !descs)) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
     if (count > b->max_stripes) return set_err(err, SCRS_ERR_CAPACITY, count, b->max_stripes);
+    int32_t rw = wait_last_run(b, async_stream, stream, err);
+    if (rw) return rw;
     // ---- validate and size the arena: [encode coefficient tables][decode slots]
     size_t coef_bytes = 0, slot_bytes = 0;
     std::map<std::tuple<int, uint32_t, uint32_t>, size_t> coef_off;
@@ -342,8 +373,7 @@ int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc
             h += (u.bytes + 15) & ~(size_t)15;
         }
     } else {
-        for (auto& u : ups)
-            if (u.bytes) SCRS_CUDA(cudaMemcpy(u.dst, u.src, u.bytes, cudaMemcpyHostToDevice));
+        for (auto& u : ups) SCRS_CUDA(upload_now(u.dst, u.src, u.bytes));
     }
     b->host_mode = false;  // scrs_stripe_batch_set_host re-enables it after this call
     if (b->graph) {  // geometry changed: the captured graph no longer applies
@@ -357,6 +387,8 @@ extern "C" int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* b, const scrs_s
                                               uint64_t count, scrs_error* err) {
     if (!b || (count && !descs)) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
     if (count > b->max_stripes) return set_err(err, SCRS_ERR_CAPACITY, count, b->max_stripes);
+    int32_t rw = wait_last_run(b, false, nullptr, err);  // the staging below may be reallocated
+    if (rw) return rw;
     size_t in_bytes = 0, out_bytes = 0;
     for (uint64_t s = 0; s < count; s++) {
         const scrs_stripe_desc& d = descs[s];
@@ -577,7 +609,7 @@ int32_t run_host(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
     }
     SCRS_CUDA(cudaEventRecord(ev_end, b->s_out));
     SCRS_CUDA(cudaStreamWaitEvent(st, ev_end, 0));
-    return set_err(err, SCRS_OK);
+    return ran_on(b, st, err);
 }
 
 }  // namespace
@@ -593,7 +625,7 @@ extern "C" int32_t scrs_stripe_batch_run(scrs_stripe_batch* b, void* stream, int
         if (r) return r;
         r = copy_out(b, st, err);
         if (r) return r;
-        return set_err(err, SCRS_OK);
+        return ran_on(b, st, err);
     }
     if (b->graph && b->graph_version != tune_version()) {  // launch parameters may have changed
         cudaGraphExecDestroy(b->graph);
@@ -626,7 +658,7 @@ extern "C" int32_t scrs_stripe_batch_run(scrs_stripe_batch* b, void* stream, int
     b->last_launches = b->graph_launches;
     r0 = copy_out(b, st, err);
     if (r0) return r0;
-    return set_err(err, SCRS_OK);
+    return ran_on(b, st, err);
 }
 
 extern "C" int32_t scrs_stripe_batch_run_plain(scrs_stripe_batch* b, void* stream, scrs_error* err) {
@@ -646,7 +678,7 @@ extern "C" int32_t scrs_stripe_batch_run_plain(scrs_stripe_batch* b, void* strea
     }
     r0 = copy_out(b, st, err);
     if (r0) return r0;
-    return set_err(err, SCRS_OK);
+    return ran_on(b, st, err);
 }
 
 extern "C" int32_t scrs_stripe_batch_run_timed(scrs_stripe_batch* b, void* stream, float* plan_ms,

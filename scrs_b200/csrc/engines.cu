@@ -306,7 +306,7 @@ extern "C" int32_t scrs_batch_encoder_create(const scrs_profile* p, scrs_batch_e
         std::vector<uint8_t> c((size_t)p->k * p->m);
         hf::gf8_coefficients(p->engine, (uint32_t)p->k, (uint32_t)p->m, c.data());
         SCRS_CUDA(e->coef.ensure(c.size()));
-        SCRS_CUDA(cudaMemcpy(e->coef.p, c.data(), c.size(), cudaMemcpyHostToDevice));
+        SCRS_CUDA(upload_now(e->coef.p, c.data(), c.size(), e->stream.s));
     }
     *out = e.release();
     return set_err(err, SCRS_OK);
@@ -494,7 +494,7 @@ extern "C" int32_t scrs_decoder_create(const scrs_profile* p, scrs_decoder** out
         d->tower.host_powers.resize(n);
         hf::tower_powers((uint32_t)n, d->tower.host_powers.data());
         SCRS_CUDA(d->tower.powers.ensure(n * 2));
-        SCRS_CUDA(cudaMemcpy(d->tower.powers.p, d->tower.host_powers.data(), n * 2, cudaMemcpyHostToDevice));
+        SCRS_CUDA(upload_now(d->tower.powers.p, d->tower.host_powers.data(), n * 2, d->stream.s));
     }
     if (p->engine == SCRS_ENGINE_AFFT) {
         d->afft.reset(new (std::nothrow) AfftCodec());
@@ -1038,12 +1038,12 @@ extern "C" int32_t scrs_incremental_encoder_create(const scrs_profile* p, scrs_i
         hf::tower_powers((uint32_t)(k + m), pw.data());
         hf::tower_coefficients((uint32_t)k, (uint32_t)m, pw.data(), c.data());
         SCRS_CUDA(e->coef.ensure(c.size() * 2));
-        SCRS_CUDA(cudaMemcpy(e->coef.p, c.data(), c.size() * 2, cudaMemcpyHostToDevice));
+        SCRS_CUDA(upload_now(e->coef.p, c.data(), c.size() * 2, e->stream.s));
     } else {
         std::vector<uint8_t> c(k * m);
         hf::gf8_coefficients(p->engine, (uint32_t)k, (uint32_t)m, c.data());
         SCRS_CUDA(e->coef.ensure(c.size()));
-        SCRS_CUDA(cudaMemcpy(e->coef.p, c.data(), c.size(), cudaMemcpyHostToDevice));
+        SCRS_CUDA(upload_now(e->coef.p, c.data(), c.size(), e->stream.s));
     }
     SCRS_CUDA(e->repairs.ensure(m * L));
     SCRS_CUDA(cudaMemset(e->repairs.p, 0, m * L));

@@ -142,7 +142,7 @@ struct Compiled {
     std::vector<char> cubin;
     cudaLibrary_t lib = nullptr;
     cudaKernel_t kernel = nullptr;
-    uint64_t attr_done = 0;  // devices whose shared-memory limit is set
+    std::atomic<uint64_t> attr_done{0};  // devices whose shared-memory limit is set
     int ctas_per_sm = 0;
 };
 
@@ -244,16 +244,14 @@ int32_t jit_kernel(int32_t engine, uint32_t k, uint32_t m, bool load_it, JitKern
     int32_t rc = load(c, err);
     if (rc) return rc;
     const int smem = (int)(kSmemHeader + (size_t)k * FieldGeom<0>::kChunk);
-    if (first_on_device(c.attr_done)) {
-        cudaError_t e = cudaFuncSetAttribute((const void*)c.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.ctas_per_sm, (const void*)c.kernel, kThreads, smem);
-        if (e != cudaSuccess) {
-            c.attr_done = 0;
-            return set_err(err, SCRS_ERR_CUDA, (uint64_t)e, __LINE__);
-        }
+    const cudaError_t e = once_per_device(c.attr_done, [&] {
+        cudaError_t r = cudaFuncSetAttribute((const void*)c.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (r == cudaSuccess)
+            r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.ctas_per_sm, (const void*)c.kernel, kThreads, smem);
         if (c.ctas_per_sm < 1) c.ctas_per_sm = 1;
-    }
+        return r;
+    });
+    if (e != cudaSuccess) return set_err(err, SCRS_ERR_CUDA, (uint64_t)e, __LINE__);
     if (out) {
         out->kernel = (const void*)c.kernel;
         out->smem = smem;

@@ -5,21 +5,33 @@
 #ifndef __CUDACC_RTC__  // the run-time compiler (jit.cu) sees only the device parts
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <atomic>
+#include <mutex>
 #endif
 
 namespace scrs {
 
 #ifndef __CUDACC_RTC__
-// Per-device one-time set-up flags (function attributes such as the dynamic
-// shared-memory limit are set per device): true the first time it is called
-// for the current device, false afterwards.
-inline bool first_on_device(uint64_t& done_mask) {
+// Per-device one-time set-up (function attributes such as the dynamic
+// shared-memory limit are set per device): runs `set` for the current device
+// until it succeeds once.  The device's bit in `done_mask` is published only
+// after `set` succeeded, and set-up runs under a lock, so no thread launches
+// on a half-set-up device.
+template <class F>
+cudaError_t once_per_device(std::atomic<uint64_t>& done_mask, F&& set) {
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return true;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return set();
     const uint64_t bit = 1ull << dev;
-    if (done_mask & bit) return false;
-    done_mask |= bit;
-    return true;
+    if (done_mask.load(std::memory_order_acquire) & bit) return cudaSuccess;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done_mask.load(std::memory_order_relaxed) & bit) return cudaSuccess;
+    e = set();
+    if (e == cudaSuccess) done_mask.fetch_or(bit, std::memory_order_release);
+    return e;
 }
 #endif
 

@@ -575,25 +575,25 @@ __global__ void __launch_bounds__(32 * kPlanWarps) cauchy_plan_warp_kernel(const
 }
 
 // Constant tables are per device: upload once on each device used.
-bool g_tables_uploaded[64] = {};
 
 cudaError_t ensure_tables() {
-    int dev = 0;
-    cudaError_t e0 = cudaGetDevice(&dev);
-    if (e0 != cudaSuccess) return e0;
-    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (g_tables_uploaded[dev]) return cudaSuccess;
-    uint8_t ex[255], lg[256] = {0};
-    uint8_t v = 1;
-    for (int i = 0; i < 255; i++) {
-        ex[i] = v;
-        lg[v] = (uint8_t)i;
-        v = gf8_mul_ce(v, 3);
-    }
-    cudaError_t e = cudaMemcpyToSymbol(c_gf8_exp, ex, sizeof ex);
-    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_gf8_log, lg, sizeof lg);
-    if (e == cudaSuccess) g_tables_uploaded[dev] = true;
-    return e;
+    static std::atomic<uint64_t> done{0};
+    return once_per_device(done, [] {
+        uint8_t ex[255], lg[256] = {0};
+        uint8_t v = 1;
+        for (int i = 0; i < 255; i++) {
+            ex[i] = v;
+            lg[v] = (uint8_t)i;
+            v = gf8_mul_ce(v, 3);
+        }
+        // complete on the device before any plan kernel (on a non-blocking stream) reads it
+        cudaError_t e = cudaMemcpyToSymbolAsync(c_gf8_exp, ex, sizeof ex, 0, cudaMemcpyHostToDevice,
+                                                cudaStreamPerThread);
+        if (e == cudaSuccess)
+            e = cudaMemcpyToSymbolAsync(c_gf8_log, lg, sizeof lg, 0, cudaMemcpyHostToDevice, cudaStreamPerThread);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamPerThread);
+        return e;
+    });
 }
 
 // Shared memory of a launch staging seg_rows input rows per segment.
@@ -607,18 +607,19 @@ size_t smem_bytes(int gf16, int seg_rows) {
 template <int kGf16>
 cudaError_t set_mxk_attrs() {
     using G = FieldGeom<kGf16>;
-    static uint64_t done = 0;
-    if (!first_on_device(done)) return cudaSuccess;
-    const int smem = (int)smem_bytes(kGf16, G::kSegMax);
-    cudaError_t e = cudaFuncSetAttribute(mxk_single_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(mxk_ksplit_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if constexpr (!kGf16) {  // the persistent drain serves GF(256) stripe batches
+    static std::atomic<uint64_t> done{0};
+    return once_per_device(done, [] {
+        const int smem = (int)smem_bytes(kGf16, G::kSegMax);
+        cudaError_t e =
+            cudaFuncSetAttribute(mxk_single_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(mxk_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    }
-    if (e != cudaSuccess) done = 0;
-    return e;
+            e = cudaFuncSetAttribute(mxk_ksplit_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if constexpr (!kGf16) {  // the persistent drain serves GF(256) stripe batches
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(mxk_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        }
+        return e;
+    });
 }
 
 // Input-split launch (see mxk_ksplit_kernel): outputs are zeroed first unless

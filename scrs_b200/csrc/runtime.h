@@ -124,6 +124,17 @@ struct OwnedStream {
 
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+// Upload of set-up data from pageable host memory, complete on the device
+// when this returns.  A plain cudaMemcpy from pageable memory may return once
+// the bytes are staged, before the DMA has landed, and the kernels that read
+// these buffers run on non-blocking streams that are not ordered after it.
+inline cudaError_t upload_now(void* dst, const void* src, size_t bytes, cudaStream_t st = cudaStreamPerThread) {
+    if (bytes == 0) return cudaSuccess;
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e;
+}
+
 inline uint32_t chunk_bytes(bool gf16) { return gf16 ? (uint32_t)FieldGeom<1>::kChunk : (uint32_t)FieldGeom<0>::kChunk; }
 
 inline uint32_t n_chunks(uint64_t L, bool gf16) {

@@ -180,7 +180,7 @@ int32_t resident(scrs_server* s, Slot& sl, const scrs_profile& p, int32_t op, Re
             hf::tower_powers((uint32_t)(p.k + p.m), pw.data());
             hf::tower_coefficients((uint32_t)p.k, (uint32_t)p.m, pw.data(), c.data());
             SCRS_CUDA(R->tower_coef.ensure(c.size() * 2));
-            SCRS_CUDA(cudaMemcpy(R->tower_coef.p, c.data(), c.size() * 2, cudaMemcpyHostToDevice));
+            SCRS_CUDA(upload_now(R->tower_coef.p, c.data(), c.size() * 2, sl.stream.s));
         } else if (need_enc) {
             rc = scrs_batch_encoder_create(&p, &R->enc, err);
             if (!rc) rc = scrs_batch_encoder_scratch(R->enc, &R->enc_s, err);

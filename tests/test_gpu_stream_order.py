@@ -150,3 +150,36 @@ def test_legacy_stream_entry_points_order_with_the_default_stream(gpu, oracle):
     dec.finalize_into_with(out, dec.scratch())
     assert np.array_equal(out, data)
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_stripe_batch_set_waits_for_the_last_run(gpu, oracle, graph):
+    """Run a batch on a held-back stream, then set the same batch object to
+    other stripes at once and run them on another stream: the first run must
+    still compute its own stripes (the set waits for it before rewriting the
+    device descriptors)."""
+    torch = _torch()
+    from scrs_b200.batch import StripeBatch
+
+    from scenarios import device_stripes, make_mixed_batch
+
+    specs1, rng1 = make_mixed_batch(torch, 48, 31, lens=(1024, 4096))
+    specs2, rng2 = make_mixed_batch(torch, 48, 32, lens=(1024, 4096))
+    st1, outs1, exp1, keep1 = device_stripes(torch, oracle, specs1, rng1)
+    st2, outs2, exp2, keep2 = device_stripes(torch, oracle, specs2, rng2)
+    torch.cuda.synchronize()
+    b = StripeBatch(gpu.lib, 64)
+    held, other = torch.cuda.Stream(), torch.cuda.Stream()
+    b.set(st1)
+    with torch.cuda.stream(held):
+        torch.cuda._sleep(HOLD_CYCLES)
+        b.run(graph=graph)
+    b.set(st2)
+    with torch.cuda.stream(other):
+        b.run(graph=graph)
+    torch.cuda.synchronize()
+    b.check()
+    for o, e in zip(outs1, exp1):
+        assert np.array_equal(o.cpu().numpy(), e)
+    for o, e in zip(outs2, exp2):
+        assert np.array_equal(o.cpu().numpy(), e)
