@@ -411,8 +411,8 @@ RATES_PER_S = (2500.0, 5000.0, 10000.0)  # offered Poisson arrival rates of the 
 def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C250005):
     """Config 5: Poisson arrivals of mixed encode/decode requests over all four
     engines through the serving loop (scrs_server_*), 64 GB budget, 8 slots.
-    The closed-loop capacity (2000 requests submitted at once, median of three
-    passes) is reported beside a sweep of fixed Poisson rates, so that runs on
+    The closed-loop capacity (2000 requests submitted at once, median of five
+    passes after a warm-up pass) is reported beside a sweep of fixed Poisson rates, so that runs on
     different hosts compare at the same offered load.  Payloads are seeded random device bytes (decode requests decode
     random received rows: the same work; bit-exactness is covered by the
     serving tests).  Latency = completion seen by the host - submit."""
@@ -447,27 +447,34 @@ def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C25
             idx = np.asarray(idx, dtype=np.uint64)
         templates.append((op, engine, k, m, Ls, d_in, d_out, idx))
     srv = Server(api.lib, 64 << 30, slots=8)
+    # start-up: the tower and additive-FFT profiles' engines resident on every slot
+    for op, engine, k, m, Ls, _, _, _ in templates:
+        if engine in (Engine.TOWER, Engine.AFFT):
+            srv.reserve(op, engine, k, m, Ls)
 
     def submit(t, tag):
         op, engine, k, m, Ls, d_in, d_out, idx = templates[t]
         srv.submit(op, engine, k, m, Ls, d_in.data_ptr(), d_out.data_ptr(), idx, tag=tag)
 
-    # warm the resident engines on every slot (building engines allocates device
-    # memory, a one-time cost per profile and slot), then the closed-loop capacity
+    # warm the slots' stripe-batch buffers (a closed-loop pass coalesces larger
+    # GF(256) groups than the template rounds, and the buffers grow, allocating,
+    # until they fit), then the closed-loop capacity
     for _ in range(8):
         for t in range(len(templates)):
             submit(t, t)
         srv.drain(600)
-    passes = []  # closed loop: 3 passes of 2000 requests submitted at once, median kept
-    for _ in range(3):
+    passes = []  # closed loop: one warm-up pass, then 5 passes of 2000 requests submitted at once, median kept
+    for p in range(6):
         order = rng.integers(0, len(templates), 2000)
         t0 = time.perf_counter()
         for t in order:
             submit(int(t), int(t))
         srv.drain(600)
         cap_s = time.perf_counter() - t0
-        passes.append((len(order) / cap_s, sum(templates[int(t)][2] * templates[int(t)][4] for t in order) / cap_s))
-    cap_rate, cap_gbps = sorted(passes)[1]
+        if p:
+            passes.append((len(order) / cap_s,
+                           sum(templates[int(t)][2] * templates[int(t)][4] for t in order) / cap_s))
+    cap_rate, cap_gbps = sorted(passes)[len(passes) // 2]
     res = {"workload": "Poisson arrivals; 70% GF(256) (Standard/Good, k~U[4,64], m~U[1,16], L in {1,4,16,64} KiB), "
                        "15% tower (k<=1024, m<=256), 15% AFFT (k<=16384, m<=16384, L 256-2048); half encode, half "
                        "decode with random erasures <= m; 64 GB budget, 8 slots, GF(256) coalesced per slot",

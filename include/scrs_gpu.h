@@ -530,6 +530,16 @@ SCRS_API int32_t scrs_server_submit(scrs_server* server, const scrs_request* req
 SCRS_API int32_t scrs_server_progress(scrs_server* server, scrs_completion* done,
                                       uint32_t capacity, uint32_t* n_done,
                                       scrs_error* err);
+/* Build the resident engines of one tower or additive-FFT profile for `op`
+ * on every slot, so that no request of that profile pays the build (device
+ * allocations, which stall the whole device) on its way through.  For
+ * start-up: SCRS_ERR_BAD_ARGUMENT (a = 3) while any slot is running
+ * requests, (a = 1) for a GF(256) engine (its stripe batches need no
+ * resident engines).  Resident engines count against the memory budget and
+ * each slot keeps at most 8 profiles, least recently used evicted first. */
+SCRS_API int32_t scrs_server_reserve(scrs_server* server, int32_t op, int32_t engine,
+                                     uint64_t k, uint64_t m, uint64_t symbol_len,
+                                     scrs_error* err);
 /* Requests queued, running or completed but not yet returned. */
 SCRS_API uint64_t scrs_server_pending(const scrs_server* server);
 SCRS_API int32_t scrs_server_get_stats(const scrs_server* server, scrs_server_stats* out);

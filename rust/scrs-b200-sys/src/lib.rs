@@ -262,6 +262,7 @@ extern "C" {
     pub fn scrs_server_destroy(server: *mut scrs_server);
     pub fn scrs_server_submit(server: *mut scrs_server, req: *const scrs_request, ticket: *mut u64, err: *mut scrs_error) -> i32;
     pub fn scrs_server_progress(server: *mut scrs_server, done: *mut scrs_completion, capacity: u32, n_done: *mut u32, err: *mut scrs_error) -> i32;
+    pub fn scrs_server_reserve(server: *mut scrs_server, op: i32, engine: i32, k: u64, m: u64, symbol_len: u64, err: *mut scrs_error) -> i32;
     pub fn scrs_server_pending(server: *const scrs_server) -> u64;
     pub fn scrs_server_get_stats(server: *const scrs_server, out: *mut scrs_server_stats) -> i32;
 }

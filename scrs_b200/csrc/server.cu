@@ -454,6 +454,24 @@ extern "C" int32_t scrs_server_progress(scrs_server* s, scrs_completion* done, u
     return set_err(err, SCRS_OK);
 }
 
+extern "C" int32_t scrs_server_reserve(scrs_server* s, int32_t op, int32_t engine, uint64_t k, uint64_t m,
+                                       uint64_t symbol_len, scrs_error* err) {
+    if (!s) return set_err(err, SCRS_ERR_NULL_ARGUMENT);
+    if (op != SCRS_OP_ENCODE && op != SCRS_OP_DECODE) return set_err(err, SCRS_ERR_BAD_ARGUMENT, 2);
+    scrs_profile p{};
+    int32_t rc = scrs_profile_resolve(engine, k, m, symbol_len, &p, err);
+    if (rc) return rc;
+    if (is_gf256(p.engine)) return set_err(err, SCRS_ERR_BAD_ARGUMENT, 1);
+    for (auto& sl : s->slots)  // engines in use must not be evicted
+        if (sl->busy) return set_err(err, SCRS_ERR_BAD_ARGUMENT, 3);
+    for (auto& sl : s->slots) {
+        Resident* R = nullptr;
+        rc = resident(s, *sl, p, op, &R, err);
+        if (rc) return rc;
+    }
+    return set_err(err, SCRS_OK);
+}
+
 extern "C" uint64_t scrs_server_pending(const scrs_server* s) {
     if (!s) return 0;
     uint64_t n = s->queue.size() + s->ready.size();

@@ -62,6 +62,9 @@ def _bind(lib: Library):
                                        C.POINTER(_Error)]
     L.scrs_server_pending.restype = C.c_uint64
     L.scrs_server_pending.argtypes = [C.c_void_p]
+    L.scrs_server_reserve.restype = C.c_int32
+    L.scrs_server_reserve.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_uint64, C.c_uint64, C.c_uint64,
+                                      C.POINTER(_Error)]
     L.scrs_server_get_stats.restype = C.c_int32
     L.scrs_server_get_stats.argtypes = [C.c_void_p, C.POINTER(_Stats)]
     lib._server_bound = True
@@ -116,6 +119,13 @@ class Server:
                 out.append(Completion(c.ticket, c.tag, c.status, c.submit_ns, c.done_ns))
             if n.value < len(self._buf):
                 return out
+
+    def reserve(self, op: int, engine, k: int, m: int, symbol_len: int):
+        """Build one tower or additive-FFT profile's engines for `op` on every
+        slot (start-up; the server must be idle)."""
+        err = _Error()
+        self._lib.check(self._lib.lib.scrs_server_reserve(self._ptr, op, int(engine), k, m, symbol_len,
+                                                          C.byref(err)), err)
 
     @property
     def pending(self) -> int:

@@ -138,3 +138,42 @@ def test_inputs_written_on_held_back_streams(gpu, oracle):
     for q, r in enumerate(reqs):
         assert np.array_equal(outs[q].cpu().numpy(), r[-1]), q
     srv.close()
+
+
+def test_reserve_builds_resident_engines_at_start_up(gpu, oracle):
+    torch = pytest.importorskip("torch")
+    from scrs_b200.serving import Server
+
+    srv = Server(gpu.lib, 1 << 30, slots=3)
+    assert srv.stats()["resident_bytes"] == 0
+    srv.reserve(OP_DECODE, Engine.AFFT, 64, 64, 256)
+    srv.reserve(OP_ENCODE, Engine.TOWER, 8, 4, 1024)
+    one = srv.stats()["resident_bytes"]
+    assert one > 0
+    srv.reserve(OP_DECODE, Engine.AFFT, 64, 64, 256)  # already resident: nothing new
+    assert srv.stats()["resident_bytes"] == one
+    with pytest.raises(RuntimeFailure):  # GF(256) stripe batches need no resident engines
+        srv.reserve(OP_ENCODE, Engine.GOOD_CAUCHY, 10, 4, 4096)
+    with pytest.raises(ConfigError):
+        srv.reserve(OP_ENCODE, Engine.TOWER, 0, 4, 64)
+    # requests of reserved profiles: correct results
+    reqs = [r for r in make_requests(torch, oracle, seed=23) if (r[1], r[2], r[3], r[4]) in
+            ((Engine.AFFT, 64, 64, 256), (Engine.TOWER, 8, 4, 1024))]
+    assert reqs
+    outs = run(srv, torch, reqs, list(range(len(reqs))))
+    for o, r in zip(outs, reqs):
+        assert np.array_equal(o.cpu().numpy(), r[-1])
+    # not while a slot runs requests: hold the producer stream so the slot stays busy
+    held = torch.cuda.Stream()
+    op, engine, k, m, L, d_in, idx, exp = reqs[0]
+    out = torch.zeros(len(exp), dtype=torch.uint8, device="cuda")
+    with torch.cuda.stream(held):
+        torch.cuda._sleep(40_000_000)
+    srv.submit(op, engine, k, m, L, d_in.data_ptr(), out.data_ptr(), idx, tag=1, stream=held)
+    with pytest.raises(RuntimeFailure):
+        srv.reserve(OP_ENCODE, Engine.TOWER, 16, 4, 1024)
+    done = srv.drain()
+    assert [c.status for c in done] == [0]
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), exp)
+    srv.close()
