@@ -29,6 +29,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import gc
 import json
 import os
 import re
@@ -415,7 +416,10 @@ def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C25
     passes after a warm-up pass) is reported beside a sweep of fixed Poisson rates, so that runs on
     different hosts compare at the same offered load.  Payloads are seeded random device bytes (decode requests decode
     random received rows: the same work; bit-exactness is covered by the
-    serving tests).  Latency = completion seen by the host - submit."""
+    serving tests).  Latency = completion seen by the host - submit.  Python's
+    garbage collector is paused during the timed passes and rates: one of its
+    collections stops this polling loop for milliseconds, which would show as
+    server latency."""
     from scrs_b200.api import Engine
     from scrs_b200.serving import OP_DECODE, OP_ENCODE, Server
 
@@ -464,6 +468,8 @@ def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C25
             submit(t, t)
         srv.drain(600)
     passes = []  # closed loop: one warm-up pass, then 5 passes of 2000 requests submitted at once, median kept
+    gc.collect()
+    gc.disable()
     for p in range(6):
         order = rng.integers(0, len(templates), 2000)
         t0 = time.perf_counter()
@@ -499,6 +505,8 @@ def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C25
         res["rates"].append({"offered_per_s": round(rate, 1), "requests": n, "failed": int(sum(c.status != 0 for c in done)),
                              "goodput_GBps": round(gb / el / 1e9, 2), "p50_ms": round(float(np.percentile(lat, 50)), 3),
                              "p99_ms": round(float(np.percentile(lat, 99)), 3)})
+        gc.collect()  # between rates, outside the timed loop
+    gc.enable()
     res["stats"] = srv.stats()
     srv.close()
     return res
@@ -657,9 +665,10 @@ def run_ours(args, world, rank, local):
             peak_kind == "measured" else "fallback 6650 GB/s",
             "traffic": round(ratio * algorithmic_bytes()) if ratio else None,
             "kernel": ("persistent drain: scrs_spec_drain (encode stripes, kernel specialised to the matrix) "
-                       "then mxk_kernel<0> (decode stripes)" if enc_spec else "mxk_kernel<0> persistent drain"),
+                       "then mxk_kernel<0, true> (decode stripes; every row 16-byte aligned)" if enc_spec
+                       else "mxk_kernel<0, true> persistent drain"),
             "algorithmic_bytes_per_launch": algorithmic_bytes(), "kernel_ms": round(drain_ms, 4),
-            "parts": {"scrs_spec_drain": part(spec_bytes, spec_ms), "mxk_kernel<0>": part(gen_bytes, gen_ms)}}
+            "parts": {"scrs_spec_drain": part(spec_bytes, spec_ms), "mxk_kernel<0, true>": part(gen_bytes, gen_ms)}}
     # ---- e2e through the host-buffer batch entry point
     e2e = None
     if not args.no_e2e:
