@@ -79,7 +79,7 @@ struct scrs_stripe_batch {
     // before it rewrites the device descriptors and staging that run reads
     cudaEvent_t ran = nullptr;
     bool ran_pending = false;
-    bool all_aligned = false;  // every task's rows 16-byte aligned: the drain without unaligned paths
+    int shape = kShapeAny;  // what every task satisfies (launch_gf256_mxk): the drain without the other paths
     ~scrs_stripe_batch() {
         if (ran) cudaEventDestroy(ran);
         if (graph) cudaGraphExecDestroy(graph);
@@ -347,7 +347,11 @@ int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc
             b->max_in = gen_max_in;
         }
     }
-    b->all_aligned = std::all_of(b->tasks.begin(), b->tasks.end(), [](const MxkTask& T) { return T.aligned != 0; });
+    const bool all_aligned =
+        std::all_of(b->tasks.begin(), b->tasks.end(), [](const MxkTask& T) { return T.aligned != 0; });
+    const bool all_whole = std::all_of(b->tasks.begin(), b->tasks.end(),
+                                       [](const MxkTask& T) { return T.L % FieldGeom<0>::kChunk == 0; });
+    b->shape = !all_aligned ? kShapeAny : all_whole ? kShapeWhole : kShapeAligned;
     b->item_task.resize(item);
     for (size_t t = 0; t < b->tasks.size(); t++)
         std::fill(b->item_task.begin() + b->tasks[t].item_begin,
@@ -558,7 +562,7 @@ int32_t enqueue_drains(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err, b
         const DrainCfg c = drain_cfg(b);
         SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), b->gen_lo,
                                    b->total_items, b->d_counter.as<uint32_t>(), b->status.dev, c.seg_rows, c.grid,
-                                   st, b->all_aligned));
+                                   st, b->shape));
         b->last_launches++;
     }
     return SCRS_OK;
@@ -600,7 +604,7 @@ int32_t run_host(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
         if (P.item_hi > P.item_lo) {
             SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), P.item_lo, P.item_hi,
                                        b->d_counter.as<uint32_t>() + q, b->status.dev, c.seg_rows, c.grid, st,
-                                       b->all_aligned));
+                                       b->shape));
             b->last_launches++;
         }
         SCRS_CUDA(cudaEventRecord(ev_done, st));
@@ -754,7 +758,7 @@ int32_t time_drain(scrs_stripe_batch* b, cudaStream_t st, int seg_rows, int grid
         SCRS_CUDA(cudaEventRecord(e0, st));
         SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), b->gen_lo,
                                    b->total_items, b->d_counter.as<uint32_t>(), b->status.dev, seg_rows, grid, st,
-                                   b->all_aligned));
+                                   b->shape));
         SCRS_CUDA(cudaEventRecord(e1, st));
         SCRS_CUDA(cudaEventSynchronize(e1));
         float ms = 0;

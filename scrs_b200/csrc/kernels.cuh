@@ -100,11 +100,14 @@ struct CauchyPlanTask {
 // (zeroed before the launch) hands items out dynamically; nullptr strides
 // items by grid instead.
 // seg_rows: input rows staged per segment, 1..FieldGeom<0>::kSegMax.
-// all_aligned: every task of the range has aligned != 0, so the kernel
-// without the unaligned paths runs (less code for the instruction cache).
+// shape: what every task of the range is known to satisfy, so that a kernel
+// without the other paths runs (less code for the instruction cache):
+// kShapeAny, kShapeAligned (aligned != 0), kShapeWhole (aligned != 0 and L a
+// multiple of the row chunk, so every chunk is full).
+constexpr int kShapeAny = 0, kShapeAligned = 1, kShapeWhole = 2;
 cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
                              uint32_t* work_counter, int32_t* status, int seg_rows, int grid, cudaStream_t stream,
-                             bool all_aligned = false);
+                             int shape = kShapeAny);
 // One task by value; grid <= 0 means one CTA per row chunk (or the
 // input-split form for more than one segment of inputs, see below).
 cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream);

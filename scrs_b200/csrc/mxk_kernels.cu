@@ -151,9 +151,10 @@ __device__ __forceinline__ void output_row(const uint8_t* buf, uint32_t c, uint1
 
 // Process one item: outputs [out_lo, out_hi) of chunk `chunk` of task T.
 // When `first_issued`, the TMA copies of the first stage (segment 0) were
-// already issued into `buf` on `bar`.  kAligned: T.aligned is known to be set
-// (the unaligned paths are compiled out).  Returns false on a wait timeout.
-template <int kGf16, bool kAligned = false>
+// already issued into `buf` on `bar`.  kShape (see launch_gf256_mxk): what T
+// is known to satisfy; the paths it rules out are compiled out.  Returns
+// false on a wait timeout.
+template <int kGf16, int kShape = kShapeAny>
 __device__ bool process_item(const MxkTask& T, uint32_t chunk, uint8_t* buf, uint8_t* steps_base, uint64_t* bar,
                              uint32_t& phase, int seg_cap, int32_t* status, uint32_t out_lo, uint32_t out_hi,
                              bool first_issued, uint32_t in_lo = 0, uint32_t in_hi = 0xFFFFFFFFu,
@@ -168,8 +169,8 @@ __device__ bool process_item(const MxkTask& T, uint32_t chunk, uint8_t* buf, uin
     const uint64_t L = T.L;
     const uint64_t off = (uint64_t)chunk * G::kChunk;
     const uint32_t n_in = umin32(T.n_in, in_hi);
-    const bool aligned = kAligned || T.aligned != 0;
-    const bool full = aligned && off + G::kChunk <= L;
+    const bool aligned = kShape >= kShapeAligned || T.aligned != 0;
+    const bool full = kShape == kShapeWhole || (aligned && off + G::kChunk <= L);
     uint16_t* steps = reinterpret_cast<uint16_t*>(steps_base + warp * kStepBytes);
 
     for (uint32_t og = out_lo; og == out_lo || og < out_hi; og += kMaxOutGroup) {
@@ -245,7 +246,7 @@ __device__ bool process_item(const MxkTask& T, uint32_t chunk, uint8_t* buf, uin
 // when it is nullptr) one ahead of use, so the claim's latency is hidden.
 // Warp 0 loads the current item's descriptor and issues its first stage's
 // copies before the CTA meets at the barrier.
-template <int kGf16, bool kAligned>
+template <int kGf16, int kShape>
 __global__ void __launch_bounds__(kThreads, 8) mxk_kernel(const MxkTask* __restrict__ tasks,
                                                           const uint32_t* __restrict__ item_task,
                                                           uint32_t item_lo, uint32_t total_items,
@@ -279,13 +280,13 @@ __global__ void __launch_bounds__(kThreads, 8) mxk_kernel(const MxkTask* __restr
                 S.task[tid] = __ldg(reinterpret_cast<const uint32_t*>(tasks + __ldg(item_task + item)) + tid);
             __syncwarp();
             const MxkTask& T = *reinterpret_cast<const MxkTask*>(S.task);
-            if ((kAligned || T.aligned) && item_loads(T, 0, T.n_out))
+            if ((kShape >= kShapeAligned || T.aligned) && item_loads(T, 0, T.n_out))
                 issue_stage<kGf16>(T, item - T.item_begin, 0, umin32((uint32_t)seg_cap, T.n_in), S.buf, S.bar, tid);
         }
         __syncthreads();
         const MxkTask& T = *reinterpret_cast<const MxkTask*>(S.task);
-        const bool issued = (kAligned || T.aligned) && item_loads(T, 0, T.n_out);
-        if (!process_item<kGf16, kAligned>(T, item - T.item_begin, S.buf, S.steps, S.bar, phase, seg_cap, status, 0, T.n_out,
+        const bool issued = (kShape >= kShapeAligned || T.aligned) && item_loads(T, 0, T.n_out);
+        if (!process_item<kGf16, kShape>(T, item - T.item_begin, S.buf, S.steps, S.bar, phase, seg_cap, status, 0, T.n_out,
                                  issued))
             return;
         __syncthreads();
@@ -616,10 +617,9 @@ cudaError_t set_mxk_attrs() {
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(mxk_ksplit_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if constexpr (!kGf16) {  // the persistent drain serves GF(256) stripe batches
-            if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(mxk_kernel<kGf16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(mxk_kernel<kGf16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            for (auto fn : {mxk_kernel<kGf16, kShapeAny>, mxk_kernel<kGf16, kShapeAligned>,
+                            mxk_kernel<kGf16, kShapeWhole>})
+                if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         }
         return e;
     });
@@ -684,20 +684,22 @@ int mxk_ctas_per_sm(int seg_rows) {
     int n = 0;
     if (set_mxk_attrs<0>() != cudaSuccess) return 1;
     cudaError_t e =
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mxk_kernel<0, false>, kThreads, smem_bytes(0, seg_rows));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mxk_kernel<0, kShapeAny>, kThreads, smem_bytes(0, seg_rows));
     if (e != cudaSuccess || n < 1) n = 1;
     return n;
 }
 
 cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
                              uint32_t* counter, int32_t* status, int seg_rows, int grid, cudaStream_t stream,
-                             bool all_aligned) {
+                             int shape) {
     if (item_end <= item_lo) return cudaSuccess;
     if (seg_rows < 1 || seg_rows > FieldGeom<0>::kSegMax) return cudaErrorInvalidValue;
     cudaError_t e = set_mxk_attrs<0>();
     if (e != cudaSuccess) return e;
     if (grid <= 0 || grid > (int)(item_end - item_lo)) grid = (int)(item_end - item_lo);
-    auto fn = all_aligned ? mxk_kernel<0, true> : mxk_kernel<0, false>;
+    auto fn = shape == kShapeWhole     ? mxk_kernel<0, kShapeWhole>
+              : shape == kShapeAligned ? mxk_kernel<0, kShapeAligned>
+                                       : mxk_kernel<0, kShapeAny>;
     fn<<<grid, kThreads, smem_bytes(0, seg_rows), stream>>>(tasks, item_task, item_lo, item_end, counter, status,
                                                             seg_rows);
     return cudaGetLastError();
