@@ -665,10 +665,10 @@ def run_ours(args, world, rank, local):
             peak_kind == "measured" else "fallback 6650 GB/s",
             "traffic": round(ratio * algorithmic_bytes()) if ratio else None,
             "kernel": ("persistent drain: scrs_spec_drain (encode stripes, kernel specialised to the matrix) "
-                       "then mxk_kernel<0, 2> (decode stripes; rows 16-byte aligned, whole 2 KiB chunks)" if enc_spec
-                       else "mxk_kernel<0, 2> persistent drain"),
+                       "then mxk_kernel<0, 7> (decode stripes; rows 16-byte aligned, whole 2 KiB chunks, "
+                       "one segment)" if enc_spec else "mxk_kernel<0, 7> persistent drain"),
             "algorithmic_bytes_per_launch": algorithmic_bytes(), "kernel_ms": round(drain_ms, 4),
-            "parts": {"scrs_spec_drain": part(spec_bytes, spec_ms), "mxk_kernel<0, 2>": part(gen_bytes, gen_ms)}}
+            "parts": {"scrs_spec_drain": part(spec_bytes, spec_ms), "mxk_kernel<0, 7>": part(gen_bytes, gen_ms)}}
     # ---- e2e through the host-buffer batch entry point
     e2e = None
     if not args.no_e2e:

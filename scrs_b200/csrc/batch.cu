@@ -79,7 +79,7 @@ struct scrs_stripe_batch {
     // before it rewrites the device descriptors and staging that run reads
     cudaEvent_t ran = nullptr;
     bool ran_pending = false;
-    int shape = kShapeAny;  // what every task satisfies (launch_gf256_mxk): the drain without the other paths
+    int shape = kShapeAny;  // kShapeAligned / kShapeWhole when every task satisfies it (launch_gf256_mxk)
     ~scrs_stripe_batch() {
         if (ran) cudaEventDestroy(ran);
         if (graph) cudaGraphExecDestroy(graph);
@@ -152,6 +152,13 @@ int32_t wait_last_run(scrs_stripe_batch* b, bool async_stream, cudaStream_t stre
         SCRS_CUDA(cudaEventSynchronize(b->ran));
     b->ran_pending = false;
     return SCRS_OK;
+}
+
+// Shape flags of a generic drain launch staging seg_rows rows per segment:
+// the batch's set-time flags, plus kShapeOneSeg when every generic task fits
+// one segment (batch tasks never accumulate).
+int drain_shape(const scrs_stripe_batch* b, int seg_rows) {
+    return b->shape | ((int)b->max_in <= seg_rows ? kShapeOneSeg : 0);
 }
 
 // The end of a run on `st`: record it for the next set.
@@ -351,7 +358,7 @@ int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc
         std::all_of(b->tasks.begin(), b->tasks.end(), [](const MxkTask& T) { return T.aligned != 0; });
     const bool all_whole = std::all_of(b->tasks.begin(), b->tasks.end(),
                                        [](const MxkTask& T) { return T.L % FieldGeom<0>::kChunk == 0; });
-    b->shape = !all_aligned ? kShapeAny : all_whole ? kShapeWhole : kShapeAligned;
+    b->shape = !all_aligned ? kShapeAny : all_whole ? (kShapeAligned | kShapeWhole) : kShapeAligned;
     b->item_task.resize(item);
     for (size_t t = 0; t < b->tasks.size(); t++)
         std::fill(b->item_task.begin() + b->tasks[t].item_begin,
@@ -562,7 +569,7 @@ int32_t enqueue_drains(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err, b
         const DrainCfg c = drain_cfg(b);
         SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), b->gen_lo,
                                    b->total_items, b->d_counter.as<uint32_t>(), b->status.dev, c.seg_rows, c.grid,
-                                   st, b->shape));
+                                   st, drain_shape(b, c.seg_rows)));
         b->last_launches++;
     }
     return SCRS_OK;
@@ -604,7 +611,7 @@ int32_t run_host(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
         if (P.item_hi > P.item_lo) {
             SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), P.item_lo, P.item_hi,
                                        b->d_counter.as<uint32_t>() + q, b->status.dev, c.seg_rows, c.grid, st,
-                                       b->shape));
+                                       drain_shape(b, c.seg_rows)));
             b->last_launches++;
         }
         SCRS_CUDA(cudaEventRecord(ev_done, st));
@@ -758,7 +765,7 @@ int32_t time_drain(scrs_stripe_batch* b, cudaStream_t st, int seg_rows, int grid
         SCRS_CUDA(cudaEventRecord(e0, st));
         SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), b->gen_lo,
                                    b->total_items, b->d_counter.as<uint32_t>(), b->status.dev, seg_rows, grid, st,
-                                   b->shape));
+                                   drain_shape(b, seg_rows)));
         SCRS_CUDA(cudaEventRecord(e1, st));
         SCRS_CUDA(cudaEventSynchronize(e1));
         float ms = 0;

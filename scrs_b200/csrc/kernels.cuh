@@ -100,11 +100,13 @@ struct CauchyPlanTask {
 // (zeroed before the launch) hands items out dynamically; nullptr strides
 // items by grid instead.
 // seg_rows: input rows staged per segment, 1..FieldGeom<0>::kSegMax.
-// shape: what every task of the range is known to satisfy, so that a kernel
-// without the other paths runs (less code for the instruction cache):
-// kShapeAny, kShapeAligned (aligned != 0), kShapeWhole (aligned != 0 and L a
-// multiple of the row chunk, so every chunk is full).
-constexpr int kShapeAny = 0, kShapeAligned = 1, kShapeWhole = 2;
+// shape: flags of what every task of the range is known to satisfy, so that
+// a kernel without the other paths runs (less code for the instruction
+// cache): kShapeAligned (aligned != 0), kShapeWhole (only with kShapeAligned:
+// L a multiple of the row chunk, so every chunk is full), kShapeOneSeg
+// (n_in <= seg_rows and accumulate == 0: no partial sums carried from one
+// segment to the next).
+constexpr int kShapeAny = 0, kShapeAligned = 1, kShapeWhole = 2, kShapeOneSeg = 4;
 cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
                              uint32_t* work_counter, int32_t* status, int seg_rows, int grid, cudaStream_t stream,
                              int shape = kShapeAny);

@@ -169,8 +169,8 @@ __device__ bool process_item(const MxkTask& T, uint32_t chunk, uint8_t* buf, uin
     const uint64_t L = T.L;
     const uint64_t off = (uint64_t)chunk * G::kChunk;
     const uint32_t n_in = umin32(T.n_in, in_hi);
-    const bool aligned = kShape >= kShapeAligned || T.aligned != 0;
-    const bool full = kShape == kShapeWhole || (aligned && off + G::kChunk <= L);
+    const bool aligned = (kShape & kShapeAligned) || T.aligned != 0;
+    const bool full = (kShape & kShapeWhole) || (aligned && off + G::kChunk <= L);
     uint16_t* steps = reinterpret_cast<uint16_t*>(steps_base + warp * kStepBytes);
 
     for (uint32_t og = out_lo; og == out_lo || og < out_hi; og += kMaxOutGroup) {
@@ -233,7 +233,8 @@ __device__ bool process_item(const MxkTask& T, uint32_t chunk, uint8_t* buf, uin
             for (uint32_t j = warp; j < og_n; j += 4) {
                 if (j != (uint32_t)warp) c = lane_coef<kGf16>(T, seg, seg_n, og, j, lane);
                 const uint32_t orow_idx = T.out_rows ? T.out_rows[og + j] : og + j;
-                output_row<kGf16>(buf, c, steps, seg_n, lane, !atomic_out && (seg != in_lo || T.accumulate),
+                output_row<kGf16>(buf, c, steps, seg_n, lane,
+                                  !(kShape & kShapeOneSeg) && !atomic_out && (seg != in_lo || T.accumulate),
                                   T.out + (uint64_t)orow_idx * T.out_stride, off, L, aligned, full, atomic_out);
             }
             __syncthreads();
@@ -280,12 +281,12 @@ __global__ void __launch_bounds__(kThreads, 8) mxk_kernel(const MxkTask* __restr
                 S.task[tid] = __ldg(reinterpret_cast<const uint32_t*>(tasks + __ldg(item_task + item)) + tid);
             __syncwarp();
             const MxkTask& T = *reinterpret_cast<const MxkTask*>(S.task);
-            if ((kShape >= kShapeAligned || T.aligned) && item_loads(T, 0, T.n_out))
+            if (((kShape & kShapeAligned) || T.aligned) && item_loads(T, 0, T.n_out))
                 issue_stage<kGf16>(T, item - T.item_begin, 0, umin32((uint32_t)seg_cap, T.n_in), S.buf, S.bar, tid);
         }
         __syncthreads();
         const MxkTask& T = *reinterpret_cast<const MxkTask*>(S.task);
-        const bool issued = (kShape >= kShapeAligned || T.aligned) && item_loads(T, 0, T.n_out);
+        const bool issued = ((kShape & kShapeAligned) || T.aligned) && item_loads(T, 0, T.n_out);
         if (!process_item<kGf16, kShape>(T, item - T.item_begin, S.buf, S.steps, S.bar, phase, seg_cap, status, 0, T.n_out,
                                  issued))
             return;
@@ -606,6 +607,16 @@ size_t smem_bytes(int gf16, int seg_rows) {
     return (size_t)kSmemHeader + (size_t)seg * chunk;
 }
 
+// The persistent drain's instantiations, indexed (one segment ? 3 : 0) +
+// (whole ? 2 : aligned ? 1 : 0).
+using DrainFn = void (*)(const MxkTask*, const uint32_t*, uint32_t, uint32_t, uint32_t*, int32_t*, int);
+constexpr DrainFn kDrains[6] = {mxk_kernel<0, kShapeAny>,
+                                mxk_kernel<0, kShapeAligned>,
+                                mxk_kernel<0, kShapeAligned | kShapeWhole>,
+                                mxk_kernel<0, kShapeOneSeg>,
+                                mxk_kernel<0, kShapeOneSeg | kShapeAligned>,
+                                mxk_kernel<0, kShapeOneSeg | kShapeAligned | kShapeWhole>};
+
 template <int kGf16>
 cudaError_t set_mxk_attrs() {
     using G = FieldGeom<kGf16>;
@@ -617,8 +628,7 @@ cudaError_t set_mxk_attrs() {
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(mxk_ksplit_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if constexpr (!kGf16) {  // the persistent drain serves GF(256) stripe batches
-            for (auto fn : {mxk_kernel<kGf16, kShapeAny>, mxk_kernel<kGf16, kShapeAligned>,
-                            mxk_kernel<kGf16, kShapeWhole>})
+            for (auto fn : kDrains)
                 if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         }
         return e;
@@ -697,9 +707,8 @@ cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, ui
     cudaError_t e = set_mxk_attrs<0>();
     if (e != cudaSuccess) return e;
     if (grid <= 0 || grid > (int)(item_end - item_lo)) grid = (int)(item_end - item_lo);
-    auto fn = shape == kShapeWhole     ? mxk_kernel<0, kShapeWhole>
-              : shape == kShapeAligned ? mxk_kernel<0, kShapeAligned>
-                                       : mxk_kernel<0, kShapeAny>;
+    if (!(shape & kShapeAligned)) shape &= ~kShapeWhole;
+    const auto fn = kDrains[(shape & kShapeOneSeg ? 3 : 0) + (shape & kShapeWhole ? 2 : shape & kShapeAligned ? 1 : 0)];
     fn<<<grid, kThreads, smem_bytes(0, seg_rows), stream>>>(tasks, item_task, item_lo, item_end, counter, status,
                                                             seg_rows);
     return cudaGetLastError();
