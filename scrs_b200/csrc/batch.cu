@@ -548,7 +548,7 @@ DrainCfg drain_cfg(const scrs_stripe_batch* b) {
         c.seg_rows = std::max(1, std::min({(int)p.seg_rows, (int)b->max_in, FieldGeom<0>::kSegMax}));
         c.ctas_per_sm = (int)p.ctas_per_sm;
     }
-    const int fit = mxk_ctas_per_sm(c.seg_rows);
+    const int fit = mxk_ctas_per_sm(c.seg_rows, drain_shape(b, c.seg_rows));
     if (c.ctas_per_sm <= 0 || c.ctas_per_sm > fit) c.ctas_per_sm = fit;
     const uint32_t items = b->total_items - b->gen_lo;
     c.grid = std::max(1, std::min<int>(b->sm_count * c.ctas_per_sm, (int)std::max<uint32_t>(items, 1)));
@@ -806,7 +806,7 @@ extern "C" int32_t scrs_stripe_batch_autotune(scrs_stripe_batch* b, void* stream
     scrs_tune_params best{};
     int32_t rc = SCRS_OK;
     for (int seg : segs) {
-        const int fit = mxk_ctas_per_sm(seg);
+        const int fit = mxk_ctas_per_sm(seg, drain_shape(b, seg));
         std::vector<int> ctas{fit};
         for (int c : {(3 * fit + 3) / 4, (fit + 1) / 2}) {
             c = std::max(1, c);

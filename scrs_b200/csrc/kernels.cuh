@@ -130,7 +130,7 @@ constexpr uint32_t kPlanSmemMaxR = 12288;
 int mxk_default_seg(int max_in);
 // Most CTAs of the GF(256) persistent drain one SM holds with seg_rows rows
 // staged per segment (shared memory and registers permitting).
-int mxk_ctas_per_sm(int seg_rows);
+int mxk_ctas_per_sm(int seg_rows, int shape = kShapeAny);
 #endif  // __CUDACC_RTC__
 
 }  // namespace scrs

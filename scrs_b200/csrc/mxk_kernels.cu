@@ -247,8 +247,10 @@ __device__ bool process_item(const MxkTask& T, uint32_t chunk, uint8_t* buf, uin
 // when it is nullptr) one ahead of use, so the claim's latency is hidden.
 // Warp 0 loads the current item's descriptor and issues its first stage's
 // copies before the CTA meets at the barrier.
+// Aligned shapes fit 9 CTAs per SM without spilling (2 % faster on cfg1
+// decodes than 8); the unaligned ones keep the registers of 8.
 template <int kGf16, int kShape>
-__global__ void __launch_bounds__(kThreads, 8) mxk_kernel(const MxkTask* __restrict__ tasks,
+__global__ void __launch_bounds__(kThreads, (kShape & kShapeAligned) ? 9 : 8) mxk_kernel(const MxkTask* __restrict__ tasks,
                                                           const uint32_t* __restrict__ item_task,
                                                           uint32_t item_lo, uint32_t total_items,
                                                           uint32_t* work_counter, int32_t* status, int seg_cap) {
@@ -607,8 +609,7 @@ size_t smem_bytes(int gf16, int seg_rows) {
     return (size_t)kSmemHeader + (size_t)seg * chunk;
 }
 
-// The persistent drain's instantiations, indexed (one segment ? 3 : 0) +
-// (whole ? 2 : aligned ? 1 : 0).
+// The persistent drain's instantiations, indexed by drain_index(shape).
 using DrainFn = void (*)(const MxkTask*, const uint32_t*, uint32_t, uint32_t, uint32_t*, int32_t*, int);
 constexpr DrainFn kDrains[6] = {mxk_kernel<0, kShapeAny>,
                                 mxk_kernel<0, kShapeAligned>,
@@ -616,6 +617,11 @@ constexpr DrainFn kDrains[6] = {mxk_kernel<0, kShapeAny>,
                                 mxk_kernel<0, kShapeOneSeg>,
                                 mxk_kernel<0, kShapeOneSeg | kShapeAligned>,
                                 mxk_kernel<0, kShapeOneSeg | kShapeAligned | kShapeWhole>};
+
+int drain_index(int shape) {
+    const bool aligned = shape & kShapeAligned, whole = aligned && (shape & kShapeWhole);
+    return (shape & kShapeOneSeg ? 3 : 0) + (whole ? 2 : aligned ? 1 : 0);
+}
 
 template <int kGf16>
 cudaError_t set_mxk_attrs() {
@@ -690,11 +696,11 @@ cudaError_t launch_single_impl(const MxkTask& T, int32_t* status, int grid, cuda
 
 int mxk_default_seg(int max_in) { return std::max(1, std::min(max_in, FieldGeom<0>::kSeg)); }
 
-int mxk_ctas_per_sm(int seg_rows) {
+int mxk_ctas_per_sm(int seg_rows, int shape) {
     int n = 0;
     if (set_mxk_attrs<0>() != cudaSuccess) return 1;
     cudaError_t e =
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mxk_kernel<0, kShapeAny>, kThreads, smem_bytes(0, seg_rows));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kDrains[drain_index(shape)], kThreads, smem_bytes(0, seg_rows));
     if (e != cudaSuccess || n < 1) n = 1;
     return n;
 }
@@ -707,8 +713,7 @@ cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, ui
     cudaError_t e = set_mxk_attrs<0>();
     if (e != cudaSuccess) return e;
     if (grid <= 0 || grid > (int)(item_end - item_lo)) grid = (int)(item_end - item_lo);
-    if (!(shape & kShapeAligned)) shape &= ~kShapeWhole;
-    const auto fn = kDrains[(shape & kShapeOneSeg ? 3 : 0) + (shape & kShapeWhole ? 2 : shape & kShapeAligned ? 1 : 0)];
+    const auto fn = kDrains[drain_index(shape)];
     fn<<<grid, kThreads, smem_bytes(0, seg_rows), stream>>>(tasks, item_task, item_lo, item_end, counter, status,
                                                             seg_rows);
     return cudaGetLastError();
