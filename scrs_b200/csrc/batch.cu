@@ -79,9 +79,15 @@ struct scrs_stripe_batch {
     // before it rewrites the device descriptors and staging that run reads
     cudaEvent_t ran = nullptr;
     bool ran_pending = false;
+    // branch of a run for the specialised drains (see enqueue_batch)
+    cudaStream_t s_fork = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int shape = kShapeAny;  // kShapeAligned / kShapeWhole when every task satisfies it (launch_gf256_mxk)
     ~scrs_stripe_batch() {
         if (ran) cudaEventDestroy(ran);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (s_fork) cudaStreamDestroy(s_fork);
         if (graph) cudaGraphExecDestroy(graph);
         for (cudaEvent_t e : events) cudaEventDestroy(e);
         if (s_in) cudaStreamDestroy(s_in);
@@ -111,6 +117,9 @@ extern "C" int32_t scrs_stripe_batch_create(uint64_t max_stripes, uint64_t max_i
     SCRS_CUDA(cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, dev));
     SCRS_CUDA(b->status.init());
     SCRS_CUDA(cudaEventCreateWithFlags(&b->ran, cudaEventDisableTiming));
+    SCRS_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+    SCRS_CUDA(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
+    SCRS_CUDA(cudaStreamCreateWithFlags(&b->s_fork, cudaStreamNonBlocking));
     SCRS_CUDA(b->d_tasks.ensure(max_stripes * sizeof(MxkTask)));
     SCRS_CUDA(b->d_plans.ensure(max_stripes * sizeof(CauchyPlanTask)));
     SCRS_CUDA(b->d_counter.ensure(kMaxPieces * sizeof(uint32_t)));
@@ -575,14 +584,31 @@ int32_t enqueue_drains(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err, b
     return SCRS_OK;
 }
 
+// One run on st.  With specialised drains and a generic one, the specialised
+// drains go on a branch (s_fork, joined back before the run ends), so that
+// they overlap the plan launch and the generic drain's CTAs take the SMs the
+// specialised drains' tails leave idle; the drains touch disjoint items and
+// outputs.  Under graph capture the fork and join become graph edges.
 int32_t enqueue_batch(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
     SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, (1 + b->spec.size()) * sizeof(uint32_t), st));
     b->last_launches = 0;
+    const bool fork = !b->spec.empty() && b->total_items > b->gen_lo;
+    if (fork) {
+        SCRS_CUDA(cudaEventRecord(b->ev_fork, st));
+        SCRS_CUDA(cudaStreamWaitEvent(b->s_fork, b->ev_fork, 0));
+        int32_t r = enqueue_drains(b, b->s_fork, err, true, false);
+        if (r) return r;
+    }
     if (!b->plans.empty()) {
         SCRS_CUDA(launch_cauchy_plan(b->d_plans.as<CauchyPlanTask>(), (uint32_t)b->plans.size(), 0, b->max_plan_r, st));
         b->last_launches++;
     }
-    return enqueue_drains(b, st, err);
+    if (!fork) return enqueue_drains(b, st, err);
+    int32_t r = enqueue_drains(b, st, err, false, true);
+    if (r) return r;
+    SCRS_CUDA(cudaEventRecord(b->ev_join, b->s_fork));
+    SCRS_CUDA(cudaStreamWaitEvent(st, b->ev_join, 0));
+    return SCRS_OK;
 }
 
 // Host-buffer run: copies and compute of consecutive pieces overlap (see top).
@@ -646,6 +672,7 @@ extern "C" int32_t scrs_stripe_batch_run(scrs_stripe_batch* b, void* stream, int
         b->graph = nullptr;
     }
     if (!b->graph) {
+        SCRS_CUDA(prepare_batch_kernels());  // its one-time set-up cannot run inside the capture
         // Capture on a private stream so the legacy default stream can be used by callers.
         cudaStream_t cap;
         SCRS_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));

@@ -131,6 +131,10 @@ int mxk_default_seg(int max_in);
 // Most CTAs of the GF(256) persistent drain one SM holds with seg_rows rows
 // staged per segment (shared memory and registers permitting).
 int mxk_ctas_per_sm(int seg_rows, int shape = kShapeAny);
+// The one-time per-device set-up of the batch kernels (decode-plan tables,
+// shared-memory limits).  Must precede a stream capture of them: the set-up
+// synchronises, which a capturing thread may not do.
+cudaError_t prepare_batch_kernels();
 #endif  // __CUDACC_RTC__
 
 }  // namespace scrs

@@ -696,6 +696,12 @@ cudaError_t launch_single_impl(const MxkTask& T, int32_t* status, int grid, cuda
 
 int mxk_default_seg(int max_in) { return std::max(1, std::min(max_in, FieldGeom<0>::kSeg)); }
 
+cudaError_t prepare_batch_kernels() {
+    cudaError_t e = ensure_tables();
+    if (e == cudaSuccess) e = set_mxk_attrs<0>();
+    return e;
+}
+
 int mxk_ctas_per_sm(int seg_rows, int shape) {
     int n = 0;
     if (set_mxk_attrs<0>() != cudaSuccess) return 1;
