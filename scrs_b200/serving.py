@@ -84,9 +84,10 @@ class Server:
         self._keep = {}
 
     def close(self):
-        if self._ptr:
-            self._lib.lib.scrs_server_destroy(self._ptr)
-            self._ptr = C.c_void_p()
+        ptr = getattr(self, "_ptr", None)
+        if ptr is not None and ptr.value:
+            self._ptr = None  # no module global needed here (finalizers can run at interpreter exit)
+            self._lib.lib.scrs_server_destroy(ptr)
             self._keep.clear()
 
     def __del__(self):
