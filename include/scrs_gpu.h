@@ -260,7 +260,9 @@ SCRS_API int32_t scrs_inc_feed(scrs_incremental_encoder* enc, uint64_t index,
 /* Device-resident feed: d_data is a device pointer.  The row is copied on
  * `stream`, so the copy follows the caller's earlier work on that stream and
  * the caller may overwrite d_data with work enqueued there afterwards; later
- * calls on this handle wait for the copy. */
+ * calls on this handle wait for the copy (through an event recorded on
+ * `stream` when they start, so `stream` must stay valid until the next
+ * repair read or reset). */
 SCRS_API int32_t scrs_inc_feed_device_stream(scrs_incremental_encoder* enc, uint64_t index,
                                     const uint8_t* d_data, uint64_t data_len,
                                     void* stream, scrs_error* err);
@@ -299,7 +301,9 @@ SCRS_API int32_t scrs_dec_push(scrs_decoder* dec, uint64_t index,
  * into the decoder's payload buffer (after the caller's earlier work on
  * `stream`; the caller may overwrite d_payload with work enqueued there
  * afterwards).  The copy also waits for the reads of the last finalize, so
- * a reset decoder can be refilled while that decode still runs. */
+ * a reset decoder can be refilled while that decode still runs.  The next
+ * finalize waits for the copy through an event it records on `stream`, so
+ * `stream` must stay valid until then. */
 SCRS_API int32_t scrs_dec_push_device_stream(scrs_decoder* dec, uint64_t index,
                                     const uint8_t* d_payload, uint64_t payload_len,
                                     void* stream, scrs_push_outcome* outcome,
