@@ -128,6 +128,12 @@ typedef struct scrs_stripe_batch scrs_stripe_batch;
 SCRS_API uint32_t scrs_abi_version(void);
 /* Human-readable name of a status code. No reference counterpart. */
 SCRS_API const char* scrs_status_name(int32_t code);
+/* Device and pinned-host allocations (cudaMalloc, cudaHostAlloc) the library
+ * has made since it was loaded, from every thread.  The zero-allocation
+ * contract of the *_with calls (scrs/tests/zero_alloc.rs:48-145 counts heap
+ * allocations with a counting global allocator) is checked by reading this
+ * before and after steady-state calls. */
+SCRS_API uint64_t scrs_alloc_count(void);
 
 /* ---- profiles: selector.rs:40-88, lib.rs:85-93 -------------------------- */
 SCRS_API int32_t scrs_profile_resolve(int32_t engine, uint64_t k, uint64_t m,
@@ -236,14 +242,21 @@ SCRS_API uint64_t scrs_decode_scratch_recipe_hits(const scrs_decode_scratch* scr
  * the library.  Decodes whose recipe exceeds it (2*(3k+3r) + k*r bytes for
  * r erased data symbols) fail with SCRS_ERR_CAPACITY (a = needed, b = 16384).
  * Calls share that array: calls whose device work overlaps race and must be
- * ordered on one stream.  The first call on a device looks up the array's
- * address; make it before any stream capture on that device. */
+ * ordered on one stream.  The first call on a device does the one-time
+ * set-up there (the array's address, the decode kernels' tables and limits;
+ * it synchronises); make it before any stream capture on that device.
+ * The call returns before its device work runs, so a bounded device wait
+ * that runs out is reported through d_status, an optional caller-owned
+ * device int32 (NULL: not reported): the kernels store
+ * SCRS_ERR_DEVICE_TIMEOUT there and never clear it, so zero it before the
+ * first call and read it after synchronising `stream`. */
 SCRS_API int32_t scrs_gf256_decode_static(int32_t engine, uint64_t k,
                                           uint64_t m, uint64_t symbol_len,
                                           const uint64_t* indices,
                                           const uint8_t* d_rows, uint64_t count,
                                           uint8_t* d_out, uint64_t out_len,
-                                          void* stream, scrs_error* err);
+                                          void* stream, int32_t* d_status,
+                                          scrs_error* err);
 
 /* ---- IncrementalEncoder: selector.rs:370-429, codec.rs:122-131 ---------- */
 /* UnsupportedMode for Standard Cauchy and AFFT (selector.rs:379). */

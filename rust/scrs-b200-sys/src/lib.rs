@@ -189,6 +189,7 @@ pub struct scrs_server_stats {
 extern "C" {
     pub fn scrs_abi_version() -> u32;
     pub fn scrs_status_name(code: i32) -> *const c_char;
+    pub fn scrs_alloc_count() -> u64;
     pub fn scrs_profile_resolve(engine: i32, k: u64, m: u64, symbol_len: u64, out: *mut scrs_profile, err: *mut scrs_error) -> i32;
     pub fn scrs_profile_recommended(field: i32, k: u64, m: u64, symbol_len: u64, out: *mut scrs_profile, err: *mut scrs_error) -> i32;
     pub fn scrs_recommended_gf16_engine(k: u64, m: u64) -> i32;
@@ -211,7 +212,7 @@ extern "C" {
     pub fn scrs_selftest_wait_timeout(limit_ns: u64, err: *mut scrs_error) -> i32;
     pub fn scrs_batch_decode_scratch_recipe_hits(scratch: *const scrs_batch_decode_scratch) -> u64;
     pub fn scrs_decode_scratch_recipe_hits(scratch: *const scrs_decode_scratch) -> u64;
-    pub fn scrs_gf256_decode_static(engine: i32, k: u64, m: u64, symbol_len: u64, indices: *const u64, d_rows: *const u8, count: u64, d_out: *mut u8, out_len: u64, stream: *mut c_void, err: *mut scrs_error) -> i32;
+    pub fn scrs_gf256_decode_static(engine: i32, k: u64, m: u64, symbol_len: u64, indices: *const u64, d_rows: *const u8, count: u64, d_out: *mut u8, out_len: u64, stream: *mut c_void, d_status: *mut i32, err: *mut scrs_error) -> i32;
     pub fn scrs_incremental_encoder_create(profile: *const scrs_profile, out: *mut *mut scrs_incremental_encoder, err: *mut scrs_error) -> i32;
     pub fn scrs_incremental_encoder_destroy(enc: *mut scrs_incremental_encoder);
     pub fn scrs_incremental_encoder_profile(enc: *const scrs_incremental_encoder, out: *mut scrs_profile) -> i32;

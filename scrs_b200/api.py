@@ -209,6 +209,7 @@ _DEVICE_SIGNATURES = [
     ("dec_push_device_stream", _I32, [_P, _U64, _BUF, _U64, _P, C.POINTER(_Push), C.POINTER(_Error)]),
     ("dec_finalize_into_with_device", _I32, [_P, _BUF, _U64, _P, _P, C.POINTER(_Error)]),
     ("status_name", C.c_char_p, [_I32]),
+    ("alloc_count", _U64, []),
     ("batch_decode_scratch_recipe_hits", _U64, [_P]),
     ("decode_scratch_recipe_hits", _U64, [_P]),
 ]

@@ -56,19 +56,28 @@ struct TowerTables {
 // then present data).  Coefficients are kept in a small device-resident LRU
 // keyed by the erasure pattern (missing data indices + the repair columns
 // used), as the reference's RecipeCache (decoder/cache.rs:15-100) keeps
-// recipes: a repeated pattern skips the plan launch.
+// recipes: a repeated pattern skips the plan launch.  Every entry is sized
+// for the largest erasure count (k * rmax elements, as the reference's
+// decode scratch reserves k * max_r coefficients, tower/decoder.rs:53-78) in
+// one arena allocated at scratch creation, with its key's capacity reserved,
+// so a lookup never allocates, hit or miss (the zero-allocation contract of
+// the *_with calls, tests/zero_alloc.rs:48-145).  Large codes get fewer
+// entries: the arena holds at most kCacheArenaBytes or one entry.
 struct RecipeBufs {
     struct Entry {
         std::vector<uint16_t> key;  // r, missing[r], repairs[r]
-        DevBuf coef;                // elem[k * r]
+        void* coef = nullptr;       // elem[k * r] inside `arena`
         uint64_t last_use = 0;
+        bool used = false;
     };
     static constexpr size_t kCacheEntries = 32;
+    static constexpr size_t kCacheArenaBytes = 16u << 20;
     DevBuf lists;   // uint16: in_rows[k] pass_rows[k] out_rows[rmax] missing[rmax] repairs[rmax] present[k]
     DevBuf work;    // uint32[4*rmax] when rmax exceeds the shared-memory plan limit
+    DevBuf arena;   // entries' coefficient buffers
     std::vector<uint16_t> host;  // same layout as `lists`
     std::vector<uint16_t> probe; // the key being looked up (capacity reserved at init)
-    std::vector<std::unique_ptr<Entry>> cache;
+    std::vector<Entry> cache;
     uint64_t clock = 0, hits = 0;
     uint32_t k = 0, rmax = 0, elem = 1;
     cudaError_t init(uint32_t k_, uint32_t rmax_, uint32_t elem_) {
@@ -77,53 +86,45 @@ struct RecipeBufs {
         probe.reserve(1 + 2 * (size_t)rmax);
         cudaError_t e = lists.ensure(host.size() * sizeof(uint16_t));
         if (e == cudaSuccess && rmax > kPlanSmemMaxR) e = work.ensure((size_t)4 * rmax * sizeof(uint32_t));
-        return e;
+        if (e != cudaSuccess) return e;
+        const size_t entry = ((size_t)k * std::max<uint32_t>(rmax, 1) * elem + 255) & ~(size_t)255;
+        const size_t n = std::max<size_t>(1, std::min(kCacheEntries, kCacheArenaBytes / entry));
+        e = arena.ensure(n * entry);
+        if (e != cudaSuccess) return e;
+        cache.resize(n);
+        for (size_t i = 0; i < n; i++) {
+            cache[i].key.reserve(1 + 2 * (size_t)rmax);
+            cache[i].coef = arena.as<uint8_t>() + i * entry;
+        }
+        return cudaSuccess;
     }
     // Coefficient buffer for the pattern; *fresh says whether it must be
-    // (re)computed.  The least recently used entry is reused when full.
+    // (re)computed.  A free entry is taken first, then the least recently
+    // used one.  Reusing a buffer that a queued kernel may still read is
+    // safe: its pattern's plan and multiply ran earlier on the same stream.
     cudaError_t lookup(const std::vector<uint16_t>& missing, const std::vector<uint16_t>& repairs, void** coef,
                        bool* fresh) {
+        if (missing.size() > rmax || cache.empty()) return cudaErrorInvalidValue;
         std::vector<uint16_t>& key = probe;
         key.clear();
         key.push_back((uint16_t)missing.size());
         key.insert(key.end(), missing.begin(), missing.end());
         key.insert(key.end(), repairs.begin(), repairs.end());
-        for (auto& e : cache)
-            if (e->key == key) {
-                e->last_use = ++clock;
+        Entry* slot = nullptr;
+        for (auto& e : cache) {
+            if (e.used && e.key == key) {
+                e.last_use = ++clock;
                 hits++;
-                *coef = e->coef.p;
+                *coef = e.coef;
                 *fresh = false;
                 return cudaSuccess;
             }
-        const size_t need = (size_t)k * std::max<size_t>(missing.size(), 1) * elem;
-        Entry* slot = nullptr;
-        if (cache.size() < kCacheEntries) {
-            cache.emplace_back(new Entry());
-            slot = cache.back().get();
-        } else {
-            // the least recently used entry whose buffer is large enough, so a
-            // reuse does not reallocate (cudaFree would wait for the device)
-            for (auto& e : cache)
-                if (e->coef.bytes >= need && (!slot || e->last_use < slot->last_use)) slot = e.get();
-            if (!slot) {
-                slot = cache[0].get();
-                for (auto& e : cache)
-                    if (e->last_use < slot->last_use) slot = e.get();
-            }
-        }
-        // Reusing a buffer that a queued kernel may still read is safe: its
-        // pattern's plan and multiply ran earlier on the same stream.
-        // new buffers get room for up to 16 erasures, so later patterns fit
-        const size_t room = (size_t)k * std::min<size_t>(std::max<size_t>(rmax, 1), 16) * elem;
-        cudaError_t e = slot->coef.ensure(slot->coef.p ? need : std::max(need, room));
-        if (e != cudaSuccess) {
-            slot->key.clear();
-            return e;
+            if (!slot || (slot->used && (!e.used || e.last_use < slot->last_use))) slot = &e;
         }
         slot->key.assign(key.begin(), key.end());
+        slot->used = true;
         slot->last_use = ++clock;
-        *coef = slot->coef.p;
+        *coef = slot->coef;
         *fresh = true;
         return cudaSuccess;
     }
@@ -209,6 +210,8 @@ int32_t run_cauchy_recover(RecipeBufs& rb, int32_t engine, uint32_t k, const std
 // library
 // ===========================================================================
 extern "C" uint32_t scrs_abi_version(void) { return 0x00010000u; }
+
+extern "C" uint64_t scrs_alloc_count(void) { return g_alloc_calls.load(std::memory_order_relaxed); }
 
 extern "C" const char* scrs_status_name(int32_t code) {
     switch (code) {

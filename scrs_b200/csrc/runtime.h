@@ -6,6 +6,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <atomic>
 #include <vector>
 
 #include "../../include/scrs_gpu.h"
@@ -32,6 +33,11 @@ inline int32_t set_err(scrs_error* err, int32_t code, uint64_t a = 0, uint64_t b
         }                                                                 \
     } while (0)
 
+// Device and pinned-host allocations the library has made (cudaMalloc,
+// cudaHostAlloc), for scrs_alloc_count: every allocation goes through the
+// three helpers below.
+inline std::atomic<uint64_t> g_alloc_calls{0};
+
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
@@ -48,6 +54,7 @@ struct DevBuf {
         if (n <= bytes && p) return cudaSuccess;
         release();
         if (n == 0) n = 16;
+        g_alloc_calls.fetch_add(1, std::memory_order_relaxed);
         cudaError_t e = cudaMalloc(&p, n);
         if (e == cudaSuccess) bytes = n;
         else p = nullptr;
@@ -80,6 +87,7 @@ struct PinnedBuf {
         if (n <= bytes && p) return cudaSuccess;
         release();
         if (n == 0) n = 16;
+        g_alloc_calls.fetch_add(1, std::memory_order_relaxed);
         cudaError_t e = cudaHostAlloc(&p, n, cudaHostAllocDefault);
         if (e == cudaSuccess) bytes = n;
         else p = nullptr;
@@ -95,6 +103,7 @@ struct StatusWord {
     int32_t* host = nullptr;
     int32_t* dev = nullptr;
     cudaError_t init() {
+        g_alloc_calls.fetch_add(1, std::memory_order_relaxed);
         cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&host), 64, cudaHostAllocMapped);
         if (e != cudaSuccess) return e;
         *host = 0;
