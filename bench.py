@@ -214,6 +214,16 @@ def verify_cfg1(torch, api, w, oracle_api=None, n_check=8):
     return ok
 
 
+def bench_config(world) -> dict:
+    """The workload's description, identical in both arms' lines."""
+    return {"workload": workload(), "engine": "GoodCauchy", "k": K, "m": M, "symbol_len": L,
+            "stripes_encode": STRIPES, "stripes_decode": STRIPES, "goodput_bytes_per_step": goodput_bytes(),
+            "l2": (f"inputs {input_bytes() / 1e9:.2f} GB per GPU > 126 MB L2, no flush needed"
+                   if input_bytes() > 126 << 20 else
+                   f"inputs {input_bytes() / 1e6:.1f} MB per GPU fit in the 126 MB L2 (small case)"),
+            "parallelism": f"weak x{world}"}
+
+
 def goodput_bytes():
     return 2 * STRIPES * K * L  # k*L per encoded and per decoded stripe
 
@@ -235,9 +245,25 @@ def load_oracle():
     lib.oracle_baseline_gf256_decode.restype = C.c_double
     lib.oracle_baseline_gf256_decode.argtypes = [C.c_int32, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
                                                  C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32]
+    lib.oracle_baseline_stripes.restype = C.c_double
+    lib.oracle_baseline_stripes.argtypes = [C.c_void_p, C.c_uint64, C.c_int32, C.POINTER(C.c_int32)]
     lib.oracle_baseline_threads.restype = C.c_int32
     lib.oracle_simd_active.restype = C.c_int32
     return lib
+
+
+def host_cpu() -> dict:
+    """Model and logical CPU count of the host the CPU legs run on."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "nproc": os.cpu_count()}
 
 
 class CpuSample:
@@ -287,14 +313,75 @@ def cpu_baseline(target_s=12.0, sample_pairs=8192):
     samp.threads = all_threads
     single = samp.goodput_bytes() / float(np.mean(one)) / 1e9
     return {"value": round(samp.goodput_bytes() / dt / 1e9, 3), "unit": "GB/s", "cores": samp.threads,
-            "kind": "port", "single_core_GBps": round(single, 3),
+            "kind": "port", "single_core_GBps": round(single, 3), "cpu": host_cpu(),
             "sample": f"{samp.count} stripes encoded + {samp.count} batch-decoded (k=10 m=4 L=4096) per pass, "
                       f"{len(times)} passes in {sum(times):.1f} s on {samp.threads} threads, "
                       f"GFNI={'on' if lib.oracle_simd_active() else 'off'}, decode {'bit-exact' if ok else 'MISMATCH'}"}
 
 
+class Cpu:
+    """The CPU legs of the extras: the oracle (the CPU restatement of the
+    reference's engines, GFNI payload kernels) as a library of host-thread
+    baselines and as the Python-bound checker."""
+
+    def __init__(self):
+        from scrs_b200.api import Api, Library
+
+        self.lib = load_oracle()
+        self.api = Api(Library(ROOT / "oracle" / "_build" / "liboracle.so", prefix="oracle_", device=False))
+        self.threads = int(self.lib.oracle_baseline_threads())
+        self.gfni = bool(self.lib.oracle_simd_active())
+
+    def time_stripes(self, desc, threads, target_s, min_passes=2, max_passes=200):
+        """Median seconds of one pass of the host descriptors `desc`
+        (DESC_DTYPE, host pointers) over `threads` threads, and the pass count."""
+        st = C.c_int32()
+        times = []
+        t_end = time.perf_counter() + target_s
+        while len(times) < min_passes or (time.perf_counter() < t_end and len(times) < max_passes):
+            times.append(self.lib.oracle_baseline_stripes(desc.ctypes.data, len(desc), threads, C.byref(st)))
+            if st.value:
+                raise RuntimeError(f"oracle stripe baseline failed with status {st.value}")
+        return float(np.median(times)), len(times)
+
+    def codec_leg(self, op, engine, k, m, Ls, data, word, order, target_s=2.0):
+        """One codec geometry on the host cores: every pass runs one
+        independent stripe per host thread (the reference is single-threaded
+        per codec) encoding `data` or decoding the received rows `order` of
+        `word`; and one stripe on one thread.  Goodput counts k*L per stripe."""
+        from scrs_b200.batch import DESC_DTYPE, OP_DECODE
+
+        T = self.threads
+        if op == OP_DECODE:
+            src = np.ascontiguousarray(np.concatenate([word[i] for i in order]))
+            outs = np.zeros((T, k * Ls), np.uint8)
+            idx = np.ascontiguousarray(np.asarray(order, dtype=np.uint16))
+        else:
+            src = np.ascontiguousarray(data)
+            outs = np.zeros((T, m * Ls), np.uint8)
+            idx = None
+        desc = np.zeros(T, dtype=DESC_DTYPE)
+        desc["op"], desc["engine"], desc["k"], desc["m"], desc["symbol_len"] = op, int(engine), k, m, Ls
+        desc["in_"] = src.ctypes.data
+        desc["out"] = outs.ctypes.data + np.arange(T, dtype=np.uint64) * outs.shape[1]
+        if idx is not None:
+            desc["indices"] = idx.ctypes.data
+        t_one, _ = self.time_stripes(desc[:1], 1, target_s / 4, min_passes=1, max_passes=20)
+        t_all, passes = self.time_stripes(desc, T, target_s)
+        ok = bool(np.array_equal(outs[0], outs[-1]))
+        if op == OP_DECODE:
+            ok &= bool(np.array_equal(outs[0], data))
+        return {"GBps": round(T * k * Ls / t_all / 1e9, 3), "single_core_GBps": round(k * Ls / t_one / 1e9, 3),
+                "single_core_ms": round(t_one * 1e3, 3), "cores": T, "passes": passes, "bit_exact": ok}
+
+    def block(self, legs: dict, sample: str) -> dict:
+        return {"kind": "port", "cores": self.threads, "cpu": host_cpu(),
+                "sample": sample + f"; CPU restatement of the reference (oracle/, GFNI={'on' if self.gfni else 'off'})",
+                **legs}
+
+
 # ---------------------------------------------------------------------------
-# extras: batched vs plain (config 4), latency, tower, AFFT
+# extras: batched vs plain (config 4), latency, tower, AFFT, serving
 # ---------------------------------------------------------------------------
 
 def time_ms(torch, fn, reps):
@@ -308,11 +395,38 @@ def time_ms(torch, fn, reps):
     return s.elapsed_time(e) / reps
 
 
-def extra_mixed(torch, api):
-    """Config 4: 8192 stripes, k~U[4,64], m~U[1,16], L in {1,4,64} KiB, half encode,
-    half decode, persistent+graph vs one launch per stripe."""
+def per_call_ms(torch, fn, samples=200, warm=5):
+    """p50 / p99 of `samples` single calls, each bracketed by CUDA events on
+    the current stream and synchronised (host issue cost included)."""
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(samples):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        fn()
+        e.record()
+        e.synchronize()
+        ts.append(s.elapsed_time(e))
+    return round(float(np.percentile(ts, 50)), 4), round(float(np.percentile(ts, 99)), 4)
+
+
+def roofline_of(nbytes, ms, note):
+    peak, kind = peaks()
+    ach = nbytes / (ms / 1e3) / 1e9
+    return {"bound": "hbm", "algorithmic_bytes": int(nbytes), "ms": round(ms, 4), "achieved": round(ach, 1),
+            "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4), "peak_source": kind, "note": note}
+
+
+def extra_mixed(torch, api, cpu=None):
+    """Config 4: 8192 stripes, k~U[4,64], m~U[1,16], L in {1,4,64} KiB, half
+    encode, half decode of real codewords (up to m data symbols erased),
+    persistent+graph vs one launch per stripe.  Every decoded stripe is
+    compared with its data, every repair with a separate encode pass, and a
+    sample of each symbol length with the oracle."""
     from scrs_b200.api import Engine
-    from scrs_b200.batch import OP_DECODE, OP_ENCODE, StripeBatch
+    from scrs_b200.batch import DESC_DTYPE, OP_DECODE, OP_ENCODE, StripeBatch
 
     rng = np.random.default_rng(SEED + 4)
     n = 8192
@@ -321,25 +435,42 @@ def extra_mixed(torch, api):
     Ls = rng.choice([1024, 4096, 65536], n)
     eng = np.where(rng.integers(0, 2, n) == 1, int(Engine.STANDARD_CAUCHY), int(Engine.GOOD_CAUCHY))
     op = np.where(np.arange(n) % 2 == 0, OP_ENCODE, OP_DECODE)
-    in_sz = ks * Ls
-    out_sz = np.where(op == OP_ENCODE, ms * Ls, ks * Ls)
-    in_off = np.concatenate([[0], np.cumsum(in_sz)[:-1]])
-    out_off = np.concatenate([[0], np.cumsum(out_sz)[:-1]])
+    dec = op == OP_DECODE
+    # every stripe's codeword (k data rows, then m repair rows), one buffer
+    w_sz = (ks + ms) * Ls
+    w_off = np.concatenate([[0], np.cumsum(w_sz)[:-1]]).astype(np.uint64)
     gen = torch.Generator(device="cuda")
     gen.manual_seed(SEED + 4)
-    inbuf = torch.randint(0, 256, (int(in_sz.sum()),), dtype=torch.uint8, device="cuda", generator=gen)
-    outbuf = torch.zeros(int(out_sz.sum()), dtype=torch.uint8, device="cuda")
+    words = torch.randint(0, 256, (int(w_sz.sum()),), dtype=torch.uint8, device="cuda", generator=gen)
+    wp = np.uint64(words.data_ptr())
+    enc_pass = StripeBatch(api.lib, n)
+    enc_pass.set_arrays(np.full(n, OP_ENCODE), eng, ks, ms, Ls, wp + w_off,
+                        wp + w_off + (ks * Ls).astype(np.uint64))
+    enc_pass.run()
+    torch.cuda.synchronize()
+    del enc_pass
     idx = np.zeros((n, 64), np.uint16)
-    for s in np.nonzero(op == OP_DECODE)[0]:
+    for s in np.nonzero(dec)[0]:
         k, m = int(ks[s]), int(ms[s])
         e = int(rng.integers(0, min(k, m) + 1))
         erased = rng.choice(k, e, replace=False)
         keep = np.setdiff1d(np.arange(k), erased)
         reps = k + rng.choice(m, e, replace=False)
         idx[s, :k] = rng.permutation(np.concatenate([keep, reps]))
+    # received rows of the decode stripes, gathered on the device
+    r_sz = np.where(dec, ks * Ls, 0)
+    r_off = np.concatenate([[0], np.cumsum(r_sz)[:-1]]).astype(np.uint64)
+    rcv = torch.empty(int(r_sz.sum()), dtype=torch.uint8, device="cuda")
+    idx_d = torch.from_numpy(idx.astype(np.int64)).cuda()
+    for s in np.nonzero(dec)[0]:
+        k, m, Lx, wo, ro = int(ks[s]), int(ms[s]), int(Ls[s]), int(w_off[s]), int(r_off[s])
+        rcv[ro:ro + k * Lx].view(k, Lx).copy_(words[wo:wo + (k + m) * Lx].view(k + m, Lx)[idx_d[s, :k]])
+    out_sz = np.where(op == OP_ENCODE, ms * Ls, ks * Ls)
+    out_off = np.concatenate([[0], np.cumsum(out_sz)[:-1]]).astype(np.uint64)
+    outbuf = torch.zeros(int(out_sz.sum()), dtype=torch.uint8, device="cuda")
+    ins = np.where(dec, np.uint64(rcv.data_ptr()) + r_off, wp + w_off)
     b = StripeBatch(api.lib, n)
-    b.set_arrays(op, eng, ks, ms, Ls, inbuf.data_ptr() + in_off.astype(np.uint64),
-                 outbuf.data_ptr() + out_off.astype(np.uint64), indices=idx)
+    b.set_arrays(op, eng, ks, ms, Ls, ins, np.uint64(outbuf.data_ptr()) + out_off, indices=idx)
     goodput = float((ks * Ls).sum())
     algo = float(np.where(op == OP_ENCODE, (ks + ms) * Ls, 2 * ks * Ls).sum())
     default = b.launch_params
@@ -351,26 +482,95 @@ def extra_mixed(torch, api):
     torch.cuda.synchronize()
     t_graph = time_ms(torch, lambda: b.run(graph=True), 10)
     launches_batched = b.last_launches
+    outbuf.zero_()
     b.run_plain()
     torch.cuda.synchronize()
     t_plain = time_ms(torch, lambda: b.run_plain(), 2)
     launches_plain = b.last_launches
     b.check()
-    return {"workload": "8192 stripes, k~U[4,64], m~U[1,16], L in {1,4,64} KiB, Standard/Good mixed, half encode "
-                        "half decode (random erasures <= m)",
-            "persistent_graph_GBps": round(goodput / t_graph / 1e6, 1),
-            "plain_per_stripe_GBps": round(goodput / t_plain / 1e6, 1),
-            "speedup": round(t_plain / t_graph, 2),
-            "persistent_ms": round(t_graph, 3), "plain_ms": round(t_plain, 3),
-            "persistent_hbm_frac": round(algo / t_graph / 1e6 / peaks()[0], 3),
-            "autotune": {"default": {"seg_rows": default.seg_rows, "ctas_per_sm": default.ctas_per_sm,
-                                     "persistent_ms": round(t_default, 3)},
-                         "chosen": {"seg_rows": tuned.seg_rows, "ctas_per_sm": tuned.ctas_per_sm,
-                                    "persistent_ms": round(t_graph, 3)}},
-            "launches": {"persistent": launches_batched, "plain": launches_plain}}
+    # outputs of the plain form, then of the persistent form
+    ok = True
+    for form in ("plain", "persistent"):
+        if form == "persistent":
+            outbuf.zero_()
+            b.run(graph=True)
+        torch.cuda.synchronize()
+        for s in range(n):
+            k, m, Lx, wo, oo = int(ks[s]), int(ms[s]), int(Ls[s]), int(w_off[s]), int(out_off[s])
+            exp = words[wo:wo + k * Lx] if dec[s] else words[wo + k * Lx:wo + (k + m) * Lx]
+            if not torch.equal(outbuf[oo:oo + int(out_sz[s])], exp):
+                ok = False
+                break
+    # a sample of every symbol length against the oracle
+    checked = 0
+    if cpu is not None:
+        for Lx in (1024, 4096, 65536):
+            for want_dec in (False, True):
+                for s in np.nonzero((Ls == Lx) & (dec == want_dec))[0][:2]:
+                    k, m, wo, oo = int(ks[s]), int(ms[s]), int(w_off[s]), int(out_off[s])
+                    word = words[wo:wo + (k + m) * Lx].cpu().numpy().reshape(k + m, Lx)
+                    p = cpu.api.resolve(Engine(int(eng[s])), k, m, Lx)
+                    got = outbuf[oo:oo + int(out_sz[s])].cpu().numpy()
+                    if want_dec:
+                        exp = np.zeros(k * Lx, np.uint8)
+                        cpu.api.batch_decoder(p).decode_into([(int(i), word[i]) for i in idx[s, :k]], exp)
+                    else:
+                        exp = np.zeros(m * Lx, np.uint8)
+                        cpu.api.batch_encoder(p).encode_into(word[:k].reshape(-1), exp)
+                    ok &= bool(np.array_equal(got, exp))
+                    checked += 1
+    res = {"workload": "8192 stripes, k~U[4,64], m~U[1,16], L in {1,4,64} KiB, Standard/Good mixed, half encode "
+                       "half decode of real codewords (random erasures <= m)",
+           "persistent_graph_GBps": round(goodput / t_graph / 1e6, 1),
+           "plain_per_stripe_GBps": round(goodput / t_plain / 1e6, 1),
+           "speedup": round(t_plain / t_graph, 2),
+           "persistent_ms": round(t_graph, 3), "plain_ms": round(t_plain, 3),
+           "persistent_hbm_frac": round(algo / t_graph / 1e6 / peaks()[0], 3),
+           "roofline": roofline_of(algo, t_graph, "plan launch + persistent drain (mxk_kernel), graph replay"),
+           "autotune": {"default": {"seg_rows": default.seg_rows, "ctas_per_sm": default.ctas_per_sm,
+                                    "persistent_ms": round(t_default, 3)},
+                        "chosen": {"seg_rows": tuned.seg_rows, "ctas_per_sm": tuned.ctas_per_sm,
+                                   "persistent_ms": round(t_graph, 3)}},
+           "launches": {"persistent": launches_batched, "plain": launches_plain},
+           "bit_exact": ok, "oracle_checked_stripes": checked,
+           "checks": "every output of the plain and the persistent form against the data / a separate encode pass; "
+                     "2 encode + 2 decode stripes of each symbol length against the oracle"}
+    if cpu is not None:
+        # the first stripes of the batch (same distribution), inputs copied to the host
+        take, acc = [], 0
+        for s in range(n):
+            take.append(s)
+            acc += int(ks[s] * Ls[s])
+            if acc > 600 << 20:
+                break
+        take = np.array(take)
+        h_in, h_out, desc = [], [], np.zeros(len(take), dtype=DESC_DTYPE)
+        for q, s in enumerate(take):
+            k, m, Lx = int(ks[s]), int(ms[s]), int(Ls[s])
+            src = rcv[int(r_off[s]):int(r_off[s]) + k * Lx] if dec[s] else words[int(w_off[s]):int(w_off[s]) + k * Lx]
+            h_in.append(src.cpu().numpy())
+            h_out.append(np.zeros(int(out_sz[s]), np.uint8))
+            desc[q] = (int(op[s]), int(eng[s]), k, m, Lx, h_in[-1].ctypes.data, h_out[-1].ctypes.data,
+                       idx[s].ctypes.data if dec[s] else 0)
+        order = np.lexsort((desc["symbol_len"], desc["m"], desc["k"], desc["engine"], desc["op"]))
+        desc = desc[order]
+        gp = float(sum(int(ks[s] * Ls[s]) for s in take))
+        t_all, passes = cpu.time_stripes(desc, cpu.threads, 6.0)
+        one = desc[::max(1, len(desc) // 64)]
+        t_one, _ = cpu.time_stripes(one, 1, 1.0, min_passes=1, max_passes=3)
+        gp_one = float((one["k"].astype(np.float64) * one["symbol_len"]).sum())
+        cpu_ok = all(np.array_equal(h_out[q], outbuf[int(out_off[s]):int(out_off[s]) + int(out_sz[s])].cpu().numpy())
+                     for q, s in enumerate(take[:64]))
+        res["cpu_baseline"] = cpu.block(
+            {"value": round(gp / t_all / 1e9, 3), "unit": "GB/s", "single_core_GBps": round(gp_one / t_one / 1e9, 3),
+             "passes": passes, "bit_exact": bool(cpu_ok)},
+            f"the first {len(take)} stripes of the batch ({gp / 1e6:.0f} MB of data, mixed encode/decode), "
+            f"sorted by geometry, one contiguous range per thread; single core: every "
+            f"{max(1, len(desc) // 64)}th of them")
+    return res
 
 
-def extra_latency(torch, api):
+def extra_latency(torch, api, cpu=None):
     """Single-stripe latency of config 1 through the per-codec device entry points."""
     from scrs_b200.api import Engine
 
@@ -389,43 +589,58 @@ def extra_latency(torch, api):
     res = {}
     for name, fn in (("encode", lambda: enc.encode_into_with(data, rep, es)),
                      ("decode", lambda: dec.decode_into_with((idx, rows), out, ds))):
-        for _ in range(20):
-            fn()
-        ts = []
-        for _ in range(200):
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record()
-            fn()
-            e.record()
-            e.synchronize()
-            ts.append(s.elapsed_time(e))
-        res[f"{name}_p50_ms"] = round(float(np.percentile(ts, 50)), 4)
-        res[f"{name}_p99_ms"] = round(float(np.percentile(ts, 99)), 4)
-    assert torch.equal(out, data)
+        res[f"{name}_p50_ms"], res[f"{name}_p99_ms"] = per_call_ms(torch, fn, warm=20)
+    res["bit_exact"] = bool(torch.equal(out, data))
     res["workload"] = "one stripe k=10 m=4 L=4096, device buffers, per-call launch (encode: 1 kernel; decode: 1 kernel, the plan comes from the recipe cache after the first call)"
     return res
 
 
-RATES_PER_S = (2500.0, 5000.0, 10000.0)  # offered Poisson arrival rates of the serving sweep
+# offered Poisson arrival rates of the serving sweep, past the closed-loop capacity
+RATES_PER_S = (2500.0, 5000.0, 10000.0, 20000.0, 30000.0, 40000.0, 60000.0)
 
 
-def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C250005):
+def extra_serving(torch, api, cpu=None, seconds_per_rate=1.5, n_templates=192, seed=0x5C250005):
     """Config 5: Poisson arrivals of mixed encode/decode requests over all four
     engines through the serving loop (scrs_server_*), 64 GB budget, 8 slots.
     The closed-loop capacity (2000 requests submitted at once, median of five
-    passes after a warm-up pass) is reported beside a sweep of fixed Poisson rates, so that runs on
-    different hosts compare at the same offered load.  Payloads are seeded random device bytes (decode requests decode
-    random received rows: the same work; bit-exactness is covered by the
-    serving tests).  Latency = completion seen by the host - submit.  Python's
-    garbage collector is paused during the timed passes and rates: one of its
-    collections stops this polling loop for milliseconds, which would show as
-    server latency."""
+    passes after a warm-up pass, each pass with a host timeline) is reported
+    beside a sweep of fixed Poisson rates up to past that capacity, so that
+    runs on different hosts compare at the same offered load.  Requests are
+    192 templates of real codewords; after the sweep every template's output
+    is compared with its expected bytes (the regular entry points' result,
+    itself compared with the oracle for one template per engine).  Latency =
+    completion seen by the host - submit.  Python's garbage collector is
+    paused during the timed passes and rates: one of its collections stops
+    this polling loop for milliseconds, which would show as server latency."""
     from scrs_b200.api import Engine
+    from scrs_b200.batch import DESC_DTYPE
     from scrs_b200.serving import OP_DECODE, OP_ENCODE, Server
 
     rng = np.random.default_rng(seed)
     tower = [(64, 16, 4096), (256, 64, 1024), (1024, 256, 512), (32, 8, 65536)]
     afft = [(1024, 1024, 1024), (4096, 4096, 256), (3000, 500, 2048), (16384, 16384, 256)]
+    encoders = {}
+
+    def encode(engine, k, m, Ls, data):
+        key = (engine, k, m, Ls)
+        p = api.resolve(engine, k, m, Ls)
+        rep = torch.zeros(m * Ls, dtype=torch.uint8, device="cuda")
+        if engine == Engine.TOWER:
+            inc = encoders.get(key) or api.incremental_encoder(p)
+            encoders[key] = inc
+            inc.reset()
+            for i in range(k):
+                inc.feed(i, data[i * Ls:(i + 1) * Ls])
+            for j in range(m):
+                rep[j * Ls:(j + 1) * Ls].copy_(torch.frombuffer(bytearray(inc.repair(j)), dtype=torch.uint8))
+        else:
+            pair = encoders.get(key)
+            if pair is None:
+                e = api.batch_encoder(p)
+                pair = encoders[key] = (e, e.scratch())
+            pair[0].encode_into_with(data, rep, pair[1])
+        return rep
+
     templates = []
     for t in range(n_templates):
         u = rng.random()
@@ -441,23 +656,50 @@ def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C25
             engine = Engine.AFFT
             k, m, Ls = afft[int(rng.integers(0, len(afft)))]
         op = OP_ENCODE if rng.random() < 0.5 else OP_DECODE
-        d_in = torch.randint(0, 256, (k * Ls,), dtype=torch.uint8, device="cuda")
-        d_out = torch.empty(((m if op == OP_ENCODE else k) * Ls,), dtype=torch.uint8, device="cuda")
+        data = torch.randint(0, 256, (k * Ls,), dtype=torch.uint8, device="cuda")
+        rep = encode(engine, k, m, Ls, data)
         idx = None
-        if op == OP_DECODE:
+        if op == OP_ENCODE:
+            d_in, expect = data, rep
+        else:
             e = int(rng.integers(0, min(k, m) + 1))
             erased = set(rng.choice(k, e, replace=False).tolist()) if e else set()
             idx = [i for i in range(k) if i not in erased] + [k + j for j in rng.choice(m, e, replace=False).tolist()]
             idx = np.asarray(idx, dtype=np.uint64)
-        templates.append((op, engine, k, m, Ls, d_in, d_out, idx))
+            word = torch.cat([data.view(k, Ls), rep.view(m, Ls)])
+            d_in = word[torch.from_numpy(idx.astype(np.int64)).cuda()].reshape(-1).contiguous()
+            expect = data
+        d_out = torch.zeros(expect.numel(), dtype=torch.uint8, device="cuda")
+        templates.append((op, engine, k, m, Ls, d_in, d_out, idx, expect))
+    encoders.clear()
+    torch.cuda.synchronize()
+    # the regular entry points' repairs against the oracle, one template per engine
+    oracle_ok, oracle_checked = True, 0
+    if cpu is not None:
+        for want in (Engine.STANDARD_CAUCHY, Engine.GOOD_CAUCHY, Engine.TOWER, Engine.AFFT):
+            for op, engine, k, m, Ls, d_in, d_out, idx, expect in templates:
+                if engine == want and op == OP_ENCODE:
+                    p = cpu.api.resolve(engine, k, m, Ls)
+                    host = d_in.cpu().numpy()
+                    if engine == Engine.TOWER:
+                        inc = cpu.api.incremental_encoder(p)
+                        for i in range(k):
+                            inc.feed(i, host[i * Ls:(i + 1) * Ls])
+                        exp = np.frombuffer(b"".join(inc.repair(j) for j in range(m)), np.uint8)
+                    else:
+                        exp = np.zeros(m * Ls, np.uint8)
+                        cpu.api.batch_encoder(p).encode_into(host, exp)
+                    oracle_ok &= bool(np.array_equal(expect.cpu().numpy(), exp))
+                    oracle_checked += 1
+                    break
     srv = Server(api.lib, 64 << 30, slots=8)
     # start-up: the tower and additive-FFT profiles' engines resident on every slot
-    for op, engine, k, m, Ls, _, _, _ in templates:
+    for op, engine, k, m, Ls, *_ in templates:
         if engine in (Engine.TOWER, Engine.AFFT):
             srv.reserve(op, engine, k, m, Ls)
 
     def submit(t, tag):
-        op, engine, k, m, Ls, d_in, d_out, idx = templates[t]
+        op, engine, k, m, Ls, d_in, d_out, idx, _ = templates[t]
         srv.submit(op, engine, k, m, Ls, d_in.data_ptr(), d_out.data_ptr(), idx, tag=tag)
 
     # warm the slots' stripe-batch buffers (a closed-loop pass coalesces larger
@@ -472,20 +714,35 @@ def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C25
     gc.disable()
     for p in range(6):
         order = rng.integers(0, len(templates), 2000)
+        b0 = srv.stats()["batches"]
         t0 = time.perf_counter()
         for t in order:
             submit(int(t), int(t))
-        srv.drain(600)
+        t_sub = time.perf_counter()
+        calls, slowest = 0, 0.0
+        while srv.pending:
+            c0 = time.perf_counter()
+            srv.progress()
+            c1 = time.perf_counter()
+            calls += 1
+            slowest = max(slowest, c1 - c0)
+            if c1 - t0 > 600:
+                raise TimeoutError("closed-loop pass did not drain")
         cap_s = time.perf_counter() - t0
         if p:
-            passes.append((len(order) / cap_s,
-                           sum(templates[int(t)][2] * templates[int(t)][4] for t in order) / cap_s))
-    cap_rate, cap_gbps = sorted(passes)[len(passes) // 2]
+            passes.append({"requests_per_s": round(len(order) / cap_s, 1),
+                           "goodput_GBps": round(sum(templates[int(t)][2] * templates[int(t)][4] for t in order)
+                                                 / cap_s / 1e9, 2),
+                           "submit_ms": round((t_sub - t0) * 1e3, 2), "drain_ms": round((cap_s - (t_sub - t0)) * 1e3, 2),
+                           "progress_calls": calls, "slowest_progress_ms": round(slowest * 1e3, 2),
+                           "batches": srv.stats()["batches"] - b0})
+    med = sorted(passes, key=lambda x: x["requests_per_s"])[len(passes) // 2]
     res = {"workload": "Poisson arrivals; 70% GF(256) (Standard/Good, k~U[4,64], m~U[1,16], L in {1,4,16,64} KiB), "
                        "15% tower (k<=1024, m<=256), 15% AFFT (k<=16384, m<=16384, L 256-2048); half encode, half "
-                       "decode with random erasures <= m; 64 GB budget, 8 slots, GF(256) coalesced per slot",
-           "closed_loop": {"requests_per_s": round(cap_rate, 1), "goodput_GBps": round(cap_gbps / 1e9, 2),
-                           "passes_requests_per_s": [round(r, 1) for r, _ in passes]},
+                       "decode of real codewords with random erasures <= m; 64 GB budget, 8 slots, GF(256) coalesced "
+                       "per slot",
+           "closed_loop": {"requests_per_s": med["requests_per_s"], "goodput_GBps": med["goodput_GBps"],
+                           "passes": passes},
            "rates": []}
     for rate in RATES_PER_S:
         n = int(rate * seconds_per_rate)
@@ -502,19 +759,44 @@ def extra_serving(torch, api, seconds_per_rate=2.0, n_templates=192, seed=0x5C25
         el = time.perf_counter() - t0
         lat = np.array([c.latency_ms for c in done])
         gb = sum(templates[c.tag][2] * templates[c.tag][4] for c in done)
-        res["rates"].append({"offered_per_s": round(rate, 1), "requests": n, "failed": int(sum(c.status != 0 for c in done)),
+        res["rates"].append({"offered_per_s": round(rate, 1), "requests": n, "achieved_per_s": round(n / el, 1),
+                             "failed": int(sum(c.status != 0 for c in done)),
                              "goodput_GBps": round(gb / el / 1e9, 2), "p50_ms": round(float(np.percentile(lat, 50)), 3),
                              "p99_ms": round(float(np.percentile(lat, 99)), 3)})
         gc.collect()  # between rates, outside the timed loop
     gc.enable()
     res["stats"] = srv.stats()
     srv.close()
+    torch.cuda.synchronize()
+    outputs_ok = all(torch.equal(t[6], t[8]) for t in templates)
+    res["bit_exact"] = bool(outputs_ok and oracle_ok)
+    res["checks"] = (f"every template's output after the sweep equals its expected bytes ({len(templates)} templates); "
+                     f"{oracle_checked} encode templates' expected bytes equal the oracle's")
+    if cpu is not None:
+        # the template mix once per pass on the host cores (one contiguous range per thread)
+        h_in, h_out, desc = [], [], np.zeros(len(templates), dtype=DESC_DTYPE)
+        h_idx = []
+        for q, (op, engine, k, m, Ls, d_in, d_out, idx, expect) in enumerate(templates):
+            h_in.append(d_in.cpu().numpy())
+            h_out.append(np.zeros(expect.numel(), np.uint8))
+            h_idx.append(np.asarray(idx if idx is not None else [0], dtype=np.uint16))
+            desc[q] = (op, int(engine), k, m, Ls, h_in[-1].ctypes.data, h_out[-1].ctypes.data,
+                       h_idx[-1].ctypes.data if op == OP_DECODE else 0)
+        desc = desc[np.lexsort((desc["symbol_len"], desc["m"], desc["k"], desc["engine"], desc["op"]))]
+        gp = float((desc["k"].astype(np.float64) * desc["symbol_len"]).sum())
+        t_all, passes_cpu = cpu.time_stripes(desc, cpu.threads, 4.0, min_passes=1)
+        res["cpu_baseline"] = cpu.block(
+            {"value": round(gp / t_all / 1e9, 3), "unit": "GB/s", "passes": passes_cpu,
+             "requests_per_s": round(len(desc) / t_all, 1)},
+            f"the {len(templates)} request templates once per pass, sorted by geometry, one contiguous range "
+            "per thread (no arrivals: the host cores' throughput on the same mix)")
     return res
 
 
-def extra_tower(torch, api):
+def extra_tower(torch, api, cpu=None):
     """Config 2: Tower k=32 m=8 L=65536, incremental encode (32 feeds) + lazy decode (8 data erased)."""
     from scrs_b200.api import Engine
+    from scrs_b200.batch import OP_DECODE, OP_ENCODE
 
     k, m, Lt = 32, 8, 65536
     p = api.resolve(Engine.TOWER, k, m, Lt)
@@ -549,19 +831,48 @@ def extra_tower(torch, api):
 
     decode()
     torch.cuda.synchronize()
-    assert torch.equal(out.view(k, Lt), data)
+    ok = bool(torch.equal(out.view(k, Lt), data))
     t_enc = time_ms(torch, encode, 10)
     t_dec = time_ms(torch, decode, 10)
-    return {"workload": "Tower k=32 m=8 L=65536: 32 device feeds + repair fold; lazy decode r=8",
-            "encode_GBps": round(k * Lt / t_enc / 1e6, 1), "decode_GBps": round(k * Lt / t_dec / 1e6, 1),
-            "encode_ms": round(t_enc, 3), "decode_ms": round(t_dec, 3)}
+    e50, e99 = per_call_ms(torch, encode)
+    d50, d99 = per_call_ms(torch, decode)
+    res = {"workload": "Tower k=32 m=8 L=65536: 32 device feeds + repair fold; lazy decode r=8 (32 device pushes + "
+                       "finalize)",
+           "encode_GBps": round(k * Lt / t_enc / 1e6, 1), "decode_GBps": round(k * Lt / t_dec / 1e6, 1),
+           "encode_ms": round(t_enc, 3), "decode_ms": round(t_dec, 3),
+           "encode_p50_ms": e50, "encode_p99_ms": e99, "decode_p50_ms": d50, "decode_p99_ms": d99,
+           "roofline": {"encode": roofline_of((k + m) * Lt, t_enc, "32 feeds + one fold launch, per call"),
+                        "decode": roofline_of(2 * k * Lt, t_dec, "32 pushes + plan + multiply-XOR, per call")}}
+    if cpu is not None:
+        h_data = data.cpu().numpy().reshape(-1)
+        h_word = [w.cpu().numpy() for w in word]
+        exp = np.frombuffer(b"".join(cpu_encode_tower(cpu, p, h_data)), np.uint8)
+        ok &= bool(np.array_equal(np.concatenate(h_word[k:]), exp))
+        legs = {"encode": cpu.codec_leg(OP_ENCODE, Engine.TOWER, k, m, Lt, h_data, h_word, order),
+                "decode": cpu.codec_leg(OP_DECODE, Engine.TOWER, k, m, Lt, h_data, h_word, order)}
+        res["cpu_baseline"] = cpu.block(legs, "one stripe per host thread per pass: 32 in-order feeds + 8 repair "
+                                              "reads (encode), batch decode of the same 32 received symbols (decode)")
+        ok &= legs["encode"]["bit_exact"] and legs["decode"]["bit_exact"]
+    res["bit_exact"] = ok
+    return res
 
 
-def extra_afft(torch, api):
+def cpu_encode_tower(cpu, p, h_data):
+    inc = cpu.api.incremental_encoder(p)
+    Ls = p.symbol_len
+    for i in range(p.k):
+        inc.feed(i, h_data[i * Ls:(i + 1) * Ls])
+    return [inc.repair(j) for j in range(p.m)]
+
+
+def extra_afft(torch, api, cpu=None):
     """Config 3: additive FFT k=4096 m=4096 L=1024 and k=32768 m=16384 L=256.
-    Each time is the mean of 20 back-to-back calls between CUDA events on the
-    stream (a call's host work overlaps the device work of the calls before)."""
+    Each mean is over 20 back-to-back calls between CUDA events on the
+    stream (a call's host work overlaps the device work of the calls
+    before); p50 / p99 are over 200 single calls.  Repairs are compared with
+    the oracle's, decodes with the data."""
     from scrs_b200.api import Engine
+    from scrs_b200.batch import OP_DECODE, OP_ENCODE
 
     res = {}
     for tag, k, m, La in (("3a", 4096, 4096, 1024), ("3b", 32768, 16384, 256)):
@@ -573,6 +884,7 @@ def extra_afft(torch, api):
         enc.encode_into_with(data, rep, es)
         torch.cuda.synchronize()
         t_enc = time_ms(torch, lambda: enc.encode_into_with(data, rep, es), 20)
+        e50, e99 = per_call_ms(torch, lambda: enc.encode_into_with(data, rep, es))
         sel = np.sort(np.random.default_rng(SEED + 3).permutation(k + m)[:k])
         word = torch.cat([data.view(k, La), rep.view(m, La)])
         rows = word[torch.from_numpy(sel).cuda()].reshape(-1).contiguous()
@@ -582,19 +894,42 @@ def extra_afft(torch, api):
         sel64 = sel.astype(np.uint64)
         dec.decode_into_with((sel64, rows), out, ds)
         torch.cuda.synchronize()
-        assert torch.equal(out, data)
+        ok = bool(torch.equal(out, data))
         t_dec = time_ms(torch, lambda: dec.decode_into_with((sel64, rows), out, ds), 20)
+        d50, d99 = per_call_ms(torch, lambda: dec.decode_into_with((sel64, rows), out, ds))
         # few erasures (2 data symbols lost): the targeted path
         few = np.array(list(range(2, k)) + [k, k + 1], dtype=np.uint64)
         rows2 = word[torch.from_numpy(few.astype(np.int64)).cuda()].reshape(-1).contiguous()
+        out.zero_()
         dec.decode_into_with((few, rows2), out, ds)
         torch.cuda.synchronize()
-        assert torch.equal(out, data)
+        ok &= bool(torch.equal(out, data))
         t_few = time_ms(torch, lambda: dec.decode_into_with((few, rows2), out, ds), 20)
-        res[tag] = {"k": k, "m": m, "symbol_len": La, "encode_GBps": round(k * La / t_enc / 1e6, 2),
-                    "decode_GBps": round(k * La / t_dec / 1e6, 2), "encode_ms": round(t_enc, 3),
-                    "decode_ms": round(t_dec, 3), "decode_2_erasures_ms": round(t_few, 3),
-                    "decode_2_erasures_GBps": round(k * La / t_few / 1e6, 2)}
+        f50, f99 = per_call_ms(torch, lambda: dec.decode_into_with((few, rows2), out, ds))
+        r = {"k": k, "m": m, "symbol_len": La, "encode_GBps": round(k * La / t_enc / 1e6, 2),
+             "decode_GBps": round(k * La / t_dec / 1e6, 2), "encode_ms": round(t_enc, 3),
+             "decode_ms": round(t_dec, 3), "decode_2_erasures_ms": round(t_few, 3),
+             "decode_2_erasures_GBps": round(k * La / t_few / 1e6, 2),
+             "encode_p50_ms": e50, "encode_p99_ms": e99, "decode_p50_ms": d50, "decode_p99_ms": d99,
+             "decode_2_erasures_p50_ms": f50, "decode_2_erasures_p99_ms": f99,
+             "roofline": {"encode": roofline_of((k + m) * La, t_enc, "butterfly passes (afft_pass_kernel) + "
+                                                                     "slicing; latency-bound, see ncu summary"),
+                          "decode": roofline_of(2 * k * La, t_dec, "locator + transforms + derivative"),
+                          "ncu_summary": "profiles/afft_tower_gf16_launches.md"}}
+        if cpu is not None:
+            h_data = data.cpu().numpy()
+            h_rep = rep.cpu().numpy()
+            exp = np.zeros(m * La, np.uint8)
+            cpu.api.batch_encoder(cpu.api.resolve(Engine.AFFT, k, m, La)).encode_into(h_data, exp)
+            ok &= bool(np.array_equal(h_rep, exp))
+            h_word = list(h_data.reshape(k, La)) + list(h_rep.reshape(m, La))
+            legs = {"encode": cpu.codec_leg(OP_ENCODE, Engine.AFFT, k, m, La, h_data, h_word, None),
+                    "decode": cpu.codec_leg(OP_DECODE, Engine.AFFT, k, m, La, h_data, h_word, sel.tolist())}
+            r["cpu_baseline"] = cpu.block(legs, "one stripe per host thread per pass: block encode (encode); batch "
+                                                "decode of the same random half of the symbols (decode)")
+            ok &= legs["encode"]["bit_exact"] and legs["decode"]["bit_exact"]
+        r["bit_exact"] = ok
+        res[tag] = r
     return res
 
 
@@ -711,9 +1046,10 @@ def run_ours(args, world, rank, local):
         launches += hb.last_launches * n_e2e
     extras = {}
     if rank == 0 and not args.no_extras:
+        cpu_legs = None if args.no_cpu else Cpu()
         for name, fn in EXTRAS.items():
             try:
-                extras[name] = fn(torch, api)
+                extras[name] = fn(torch, api, cpu_legs)
             except Exception as ex:  # reported, never hidden
                 extras[name] = {"error": repr(ex)[:300]}
     if rank != 0:
@@ -724,15 +1060,11 @@ def run_ours(args, world, rank, local):
         "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8",
         "data": "synthetic: seeded uniform random bytes (torch.Generator), seeded 10-of-14 erasure sets",
-        "config": {"workload": workload(), "engine": "GoodCauchy", "k": K, "m": M, "symbol_len": L,
-                   "stripes_encode": STRIPES, "stripes_decode": STRIPES, "goodput_bytes_per_step": goodput_bytes(),
-                   "l2": (f"inputs {input_bytes() / 1e9:.2f} GB per GPU > 126 MB L2, no flush needed"
-                          if input_bytes() > 126 << 20 else
-                          f"inputs {input_bytes() / 1e6:.1f} MB per GPU fit in the 126 MB L2 (small case)"), "parallelism": f"weak x{world}",
-                   "bit_exact": ok,
-                   "drain_launch": {"seg_rows": tuned.seg_rows, "ctas_per_sm": tuned.ctas_per_sm,
-                                    "chosen_by": "scrs_stripe_batch_autotune",
-                                    "encode_stripes_on_specialised_kernel": b.jit_stripes}},
+        "config": bench_config(world),
+        "bit_exact": ok,
+        "drain_launch": {"seg_rows": tuned.seg_rows, "ctas_per_sm": tuned.ctas_per_sm,
+                         "chosen_by": "scrs_stripe_batch_autotune",
+                         "encode_stripes_on_specialised_kernel": b.jit_stripes},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk.result, "extras": extras,
     }
@@ -762,8 +1094,7 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic: seeded uniform random bytes",
-        "config": {"workload": workload(), "engine": "GoodCauchy", "k": K, "m": M, "symbol_len": L,
-                   "parallelism": f"weak x{world}"},
+        "config": bench_config(world),
         "cpu_baseline": cpu, "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                                      "d2h_bytes_per_step": 0}}))
 

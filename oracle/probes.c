@@ -188,3 +188,115 @@ double oracle_baseline_gf256_decode(int32_t engine, uint64_t k, uint64_t m, uint
     baseline_job j = {engine, 1, k, m, L, 0, 0, in, indices, out};
     return run_baseline(j, count, threads);
 }
+
+/* ---- CPU baseline over stripes of any engine and geometry ----------------- */
+/* Each thread takes a contiguous range of the descriptors (the caller sorts
+ * them by geometry so a thread rebuilds its codecs rarely) and runs them one
+ * by one through the reference's own per-engine entry points: batch encode
+ * (GF(256), AFFT) or k in-order feeds and m repair reads (tower,
+ * tower/encoder.rs:89-131), and batch decode (every engine; the GF(65536)
+ * engines through the lazy decoder, codec.rs:203-239). */
+typedef struct {
+    const scrs_stripe_desc* d;
+    uint64_t begin, end;
+    int32_t failed;
+} stripes_job;
+
+static int same_geometry(const scrs_stripe_desc* a, const scrs_stripe_desc* b) {
+    return a->op == b->op && a->engine == b->engine && a->k == b->k && a->m == b->m &&
+           a->symbol_len == b->symbol_len;
+}
+
+static void* stripes_worker(void* arg) {
+    stripes_job* j = (stripes_job*)arg;
+    const scrs_stripe_desc* cur = NULL;
+    oracle_batch_encoder* be = NULL;
+    oracle_encode_scratch* bes = NULL;
+    oracle_incremental_encoder* ie = NULL;
+    oracle_batch_decoder* bd = NULL;
+    oracle_batch_decode_scratch* bds = NULL;
+    uint64_t *idx = NULL, *lens = NULL;
+    const uint8_t** pay = NULL;
+    uint64_t cap = 0;
+    for (uint64_t i = j->begin; i < j->end && !j->failed; i++) {
+        const scrs_stripe_desc* d = &j->d[i];
+        const uint64_t k = d->k, m = d->m, L = d->symbol_len;
+        if (!cur || !same_geometry(cur, d)) {
+            oracle_encode_scratch_destroy(bes), bes = NULL;
+            oracle_batch_encoder_destroy(be), be = NULL;
+            oracle_incremental_encoder_destroy(ie), ie = NULL;
+            oracle_batch_decode_scratch_destroy(bds), bds = NULL;
+            oracle_batch_decoder_destroy(bd), bd = NULL;
+            scrs_profile p = {d->engine, 0, k, m, L};
+            int32_t rc;
+            if (d->op == SCRS_OP_DECODE) {
+                rc = oracle_batch_decoder_create(&p, &bd, NULL);
+                if (!rc) rc = oracle_batch_decoder_scratch(bd, &bds, NULL);
+            } else if (d->engine == SCRS_ENGINE_TOWER) {
+                rc = oracle_incremental_encoder_create(&p, &ie, NULL);
+            } else {
+                rc = oracle_batch_encoder_create(&p, &be, NULL);
+                if (!rc) rc = oracle_batch_encoder_scratch(be, &bes, NULL);
+            }
+            if (rc) {
+                j->failed = rc;
+                break;
+            }
+            cur = d;
+        }
+        int32_t rc = SCRS_OK;
+        if (d->op == SCRS_OP_DECODE) {
+            if (k > cap) {
+                free(idx), free(lens), free((void*)pay);
+                cap = k;
+                idx = (uint64_t*)malloc(k * sizeof(uint64_t));
+                lens = (uint64_t*)malloc(k * sizeof(uint64_t));
+                pay = (const uint8_t**)malloc(k * sizeof(uint8_t*));
+            }
+            for (uint64_t q = 0; q < k; q++) {
+                idx[q] = d->indices[q];
+                pay[q] = d->in + q * L;
+                lens[q] = L;
+            }
+            rc = oracle_batch_decode_into_with(bd, idx, pay, lens, k, d->out, k * L, bds, NULL);
+        } else if (ie) {
+            oracle_inc_reset(ie);
+            for (uint64_t q = 0; q < k && !rc; q++) rc = oracle_inc_feed(ie, q, d->in + q * L, L, NULL);
+            for (uint64_t r = 0; r < m && !rc; r++) rc = oracle_inc_repair(ie, r, d->out + r * L, L, NULL);
+        } else {
+            rc = oracle_batch_encode_into_with(be, d->in, k * L, d->out, m * L, bes, NULL);
+        }
+        if (rc) j->failed = rc;
+    }
+    free(idx), free(lens), free((void*)pay);
+    oracle_encode_scratch_destroy(bes);
+    oracle_batch_encoder_destroy(be);
+    oracle_incremental_encoder_destroy(ie);
+    oracle_batch_decode_scratch_destroy(bds);
+    oracle_batch_decoder_destroy(bd);
+    return NULL;
+}
+
+double oracle_baseline_stripes(const scrs_stripe_desc* descs, uint64_t count, int32_t threads,
+                               int32_t* status) {
+    if (threads < 1) threads = 1;
+    if ((uint64_t)threads > count) threads = count ? (int32_t)count : 1;
+    pthread_t* tids = (pthread_t*)malloc((size_t)threads * sizeof(pthread_t));
+    stripes_job* jobs = (stripes_job*)calloc((size_t)threads, sizeof(stripes_job));
+    oracle_tables_init();
+    double t0 = now_s();
+    for (int32_t t = 0; t < threads; t++) {
+        jobs[t].d = descs;
+        jobs[t].begin = count * (uint64_t)t / (uint64_t)threads;
+        jobs[t].end = count * (uint64_t)(t + 1) / (uint64_t)threads;
+        pthread_create(&tids[t], NULL, stripes_worker, &jobs[t]);
+    }
+    for (int32_t t = 0; t < threads; t++) pthread_join(tids[t], NULL);
+    double dt = now_s() - t0;
+    int32_t rc = 0;
+    for (int32_t t = 0; t < threads && !rc; t++) rc = jobs[t].failed;
+    if (status) *status = rc;
+    free(tids);
+    free(jobs);
+    return dt;
+}

@@ -126,6 +126,12 @@ double oracle_baseline_gf256_decode(int32_t engine, uint64_t k, uint64_t m, uint
                                     const uint8_t* in, const uint16_t* indices, uint8_t* out,
                                     uint64_t count, int32_t threads);
 int32_t oracle_baseline_threads(void);
+/* Runs `count` stripes of any engine and geometry (scrs_stripe_desc, every
+ * pointer in HOST memory) over `threads` host threads, each taking a
+ * contiguous range; *status gets the first failure (0 when all succeeded).
+ * Returns elapsed seconds. */
+double oracle_baseline_stripes(const scrs_stripe_desc* descs, uint64_t count, int32_t threads,
+                               int32_t* status);
 
 #ifdef __cplusplus
 }

@@ -41,7 +41,9 @@ def find(pattern, lines, rel):
 
 
 def main():
-    root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_kats.py <path to the SCRS reference checkout>")
+    root = Path(sys.argv[1])
     kats = {"source": "SCRS reference test modules (read as text)"}
 
     rel = "scrs/src/algebra/gf256.rs"

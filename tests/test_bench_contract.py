@@ -22,6 +22,7 @@ def test_reference_arm_prints_one_contract_line():
     assert d["impl"] == "reference"
     assert d["metric"] == bench.METRIC and d["unit"] == "GB/s" and d["higher_is_better"] is True
     assert d["config"]["workload"] == bench.workload()
+    assert d["config"] == bench.bench_config(1)  # the GPU arm's config, key for key
     assert d["value"] > 0 and d["steps"] == 1 and d["warmup"] >= 3
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["cores"] >= 1 and cb["kind"] in ("port", "reference") and cb["sample"]

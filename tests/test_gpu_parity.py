@@ -178,7 +178,8 @@ def test_tower_cfg2_shape(gpu, oracle):
 
 @pytest.mark.parametrize("k,m,L", [(5, 3, 6), (8, 4, 64), (3, 2, 2), (100, 20, 64), (17, 7, 130), (4, 2, 64),
                                    (16, 4, 40), (256, 64, 48), (512, 128, 40), (1, 1, 2), (8, 8, 4),
-                                   (4096, 4096, 1024), (32768, 32768, 4), (40000, 25536, 2)])
+                                   (4096, 4096, 1024), (32768, 32768, 4), (40000, 25536, 2),
+                                   (32768, 16384, 256)])
 def test_afft_encode_matches_oracle(gpu, oracle, k, m, L):
     p = gpu.resolve(Engine.AFFT, k, m, L)
     data = gfpy.rng_bytes(k * L, 17 * k + m)
@@ -214,6 +215,26 @@ def test_afft_random_and_large_patterns(gpu, oracle):
     word = encode_word(gpu, p, data)
     sel = np.random.default_rng(3).permutation(k + m)[:k].tolist()
     assert np.array_equal(lazy_decode(gpu, p, word, sel), data)
+
+
+def test_afft_cfg3b_shape(gpu, oracle):
+    """The config-3b shape (k=32768, m=16384, L=256): repairs equal the
+    oracle's, and the data comes back from a random 32768 of the 49152
+    symbols (full path) and from all but 3 data symbols (targeted path),
+    through the batch and the lazy decoders."""
+    k, m, L = 32768, 16384, 256
+    p = gpu.resolve(Engine.AFFT, k, m, L)
+    data = gfpy.rng_bytes(k * L, 0x5C25003B)
+    word = encode_word(gpu, p, data)
+    exp = np.zeros(m * L, np.uint8)
+    oracle.batch_encoder(p).encode_into(data, exp)
+    assert np.array_equal(np.concatenate(word[k:]), exp)
+    rng = np.random.default_rng(0x3B)
+    sel = rng.permutation(k + m)[:k].tolist()
+    assert np.array_equal(batch_decode(gpu, p, word, sel), data)
+    assert np.array_equal(lazy_decode(gpu, p, word, sel), data)
+    few = rng.permutation([i for i in range(k) if i not in (5, 777, 32767)] + [k + 1, k + 9000, k + m - 1]).tolist()
+    assert np.array_equal(batch_decode(gpu, p, word, few), data)
 
 
 @pytest.mark.parametrize("k,m,L", [(4096, 64, 1024), (1000, 24, 258), (37, 11, 6), (2048, 8, 4096)])

@@ -21,7 +21,8 @@ def make_requests(torch, oracle, seed=11):
     shapes = [(Engine.GOOD_CAUCHY, 10, 4, 4096), (Engine.STANDARD_CAUCHY, 6, 3, 1000),
               (Engine.GOOD_CAUCHY, 40, 16, 2048), (Engine.STANDARD_CAUCHY, 3, 2, 64),
               (Engine.TOWER, 8, 4, 1024), (Engine.TOWER, 32, 8, 4096),
-              (Engine.AFFT, 64, 64, 256), (Engine.AFFT, 100, 28, 512)]
+              (Engine.AFFT, 64, 64, 256), (Engine.AFFT, 100, 28, 512),
+              (Engine.AFFT, 16384, 16384, 256), (Engine.AFFT, 3000, 500, 2048)]
     reqs = []
     for rep in range(3):
         for engine, k, m, L in shapes:
