@@ -389,8 +389,15 @@ SCRS_API int32_t scrs_stripe_batch_set(scrs_stripe_batch* batch,
  * internal streams) while piece p computes; the run's stream waits for the
  * last copy.  Copies of stripes that are contiguous in host memory are
  * merged; a merged copy the driver refuses (host buffers that touch but are
- * separate allocations) is issued stripe by stripe instead.  use_graph is
- * ignored in this mode. */
+ * separate allocations) is issued stripe by stripe instead.  A decode
+ * stripe's present data rows are copied on the host, by the batch's worker
+ * threads, from its input rows into `out` while the GPU runs; the device
+ * computes and copies back only the missing rows (through pinned staging the
+ * batch owns), so the link carries k*L bytes in and r*L out per decode
+ * stripe with r data symbols erased (BatchCodec writes the present rows into
+ * the output the same way, batch/codec.rs:323-324).  In this mode
+ * scrs_stripe_batch_run returns once every output is in its host buffer, and
+ * use_graph is ignored. */
 SCRS_API int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* batch,
                                             const scrs_stripe_desc* descs,
                                             uint64_t count, scrs_error* err);

@@ -14,11 +14,22 @@
 // pieces of about equal input bytes; piece p's host->device copies, its plan
 // and drain launches and its device->host copies run on three streams, so the
 // copies of one piece overlap the compute of the previous one and both copy
-// directions run at once.
+// directions run at once.  A decode stripe's present data rows are already
+// in the caller's input rows: the device computes only the missing rows and
+// copies them back (compact) into pinned staging, and host worker threads
+// copy the present rows from the input rows into `out` while the GPU runs,
+// then each piece's missing rows from the staging once that piece is back.
+// The link then carries k*L in and r*L out per decode stripe instead of
+// k*L each way.
 #include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <functional>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <new>
+#include <thread>
 #include <tuple>
 
 #include "host_field.h"
@@ -27,6 +38,68 @@
 #include "tune.h"
 
 using namespace scrs;
+
+namespace {
+
+// Host worker threads of a host-buffer batch.  run(f) calls f(w) on every
+// worker w and returns when all have finished.
+class HostPool {
+   public:
+    ~HostPool() {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : threads_) t.join();
+    }
+    int size() const { return (int)threads_.size(); }
+    bool start(int n) {
+        if (!threads_.empty()) return true;
+        try {
+            for (int w = 0; w < n; w++) threads_.emplace_back([this, w] { loop(w); });
+        } catch (...) {
+            return !threads_.empty();
+        }
+        return true;
+    }
+    void run(const std::function<void(int)>& f) {
+        std::unique_lock<std::mutex> g(mu_);
+        work_ = &f;
+        remaining_ = (int)threads_.size();
+        gen_++;
+        cv_.notify_all();
+        done_cv_.wait(g, [this] { return remaining_ == 0; });
+        work_ = nullptr;
+    }
+
+   private:
+    void loop(int w) {
+        uint64_t seen = 0;
+        for (;;) {
+            const std::function<void(int)>* f;
+            {
+                std::unique_lock<std::mutex> g(mu_);
+                cv_.wait(g, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+                f = work_;
+            }
+            (*f)(w);
+            std::lock_guard<std::mutex> g(mu_);
+            if (--remaining_ == 0) done_cv_.notify_one();
+        }
+    }
+    std::vector<std::thread> threads_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void(int)>* work_ = nullptr;
+    uint64_t gen_ = 0;
+    int remaining_ = 0;
+    bool stop_ = false;
+};
+
+}  // namespace
 
 struct scrs_stripe_batch {
     uint64_t max_stripes = 0, max_items = 0;
@@ -69,12 +142,24 @@ struct scrs_stripe_batch {
         size_t h2d_lo, h2d_hi, d2h_lo, d2h_hi;
     };
     bool host_mode = false;
+    // decode stripes of a host-buffer batch (see the top of this file)
+    struct RowCopy {
+        const uint8_t* src;
+        uint8_t* dst;
+        size_t bytes;
+    };
+    bool compact_decode = false;            // set_impl builds compact decode tasks (set_host)
+    PinnedBuf h_missing;                    // the missing rows, compact, as the device returns them
+    std::vector<RowCopy> present_copies;    // caller's input row -> caller's output row
+    std::vector<RowCopy> missing_copies;    // h_missing row -> caller's output row, by piece
+    std::vector<size_t> missing_at;         // first missing copy of each piece, then the total
+    std::unique_ptr<HostPool> pool;
     DevBuf stage_in, stage_out;
     std::vector<Copy> h2d, d2h;              // merged copies
     std::vector<Copy> h2d_parts, d2h_parts;  // one per stripe
     std::vector<Piece> pieces;
     cudaStream_t s_in = nullptr, s_out = nullptr;
-    std::vector<cudaEvent_t> events;  // start, end, then per piece: copied in, computed
+    std::vector<cudaEvent_t> events;  // start, end, per piece: copied in, computed; then per piece: copied out
     // recorded on a run's stream after its work: the next set waits for it
     // before it rewrites the device descriptors and staging that run reads
     cudaEvent_t ran = nullptr;
@@ -289,8 +374,10 @@ int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc
             uint8_t* dcoef = dbase + off;
             off = align16(off + (size_t)k * std::max<uint32_t>(r, 1));
             T.in_rows = dL16;
-            T.pass_rows = dL16 + k;
-            T.out_rows = dL16 + 2 * k;
+            // compact (host-buffer batches): the r missing rows only, as rows
+            // 0..r-1 of `out`; the present rows never leave the host
+            T.pass_rows = b->compact_decode ? nullptr : dL16 + k;
+            T.out_rows = b->compact_decode ? nullptr : dL16 + 2 * k;
             T.coef = dcoef;
             T.n_out = r;
             T.ld = std::max<uint32_t>(r, 1);
@@ -411,28 +498,42 @@ extern "C" int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* b, const scrs_s
     if (count > b->max_stripes) return set_err(err, SCRS_ERR_CAPACITY, count, b->max_stripes);
     int32_t rw = wait_last_run(b, false, nullptr, err);  // the staging below may be reallocated
     if (rw) return rw;
-    size_t in_bytes = 0, out_bytes = 0;
+    // Output rows per stripe on the device: m repairs, or the r missing data
+    // rows of a decode (indices are validated by the set below; a bad list
+    // only sizes the staging here).
+    auto rows_out = [](const scrs_stripe_desc& d) -> uint64_t {
+        if (d.op != SCRS_OP_DECODE) return d.m;
+        uint64_t r = 0;
+        for (uint32_t q = 0; q < d.k; q++) r += d.indices[q] >= d.k;
+        return r;
+    };
+    size_t in_bytes = 0, out_bytes = 0, miss_bytes = 0;
     for (uint64_t s = 0; s < count; s++) {
         const scrs_stripe_desc& d = descs[s];
-        const uint64_t rows_out = d.op == SCRS_OP_ENCODE ? d.m : d.k;
+        if (!d.in || !d.out || (d.op == SCRS_OP_DECODE && !d.indices))
+            return set_err(err, SCRS_ERR_NULL_ARGUMENT, 0, s);
+        const uint64_t ob = rows_out(d) * d.symbol_len;
         in_bytes += (((uint64_t)d.k * d.symbol_len) + 15) & ~15ull;
-        out_bytes += ((rows_out * d.symbol_len) + 15) & ~15ull;
+        out_bytes += (ob + 15) & ~15ull;
+        if (d.op == SCRS_OP_DECODE) miss_bytes += (ob + 15) & ~15ull;
     }
     SCRS_CUDA(b->stage_in.ensure(in_bytes));
     SCRS_CUDA(b->stage_out.ensure(out_bytes));
+    SCRS_CUDA(b->h_missing.ensure(miss_bytes));
     std::vector<scrs_stripe_desc> dev(descs, descs + count);
     b->h2d.clear();
     b->d2h.clear();
     b->h2d_parts.clear();
     b->d2h_parts.clear();
+    b->present_copies.clear();
+    b->missing_copies.clear();
+    b->missing_at.clear();
     // piece boundaries: about equal input bytes per piece
     const size_t n_pieces = std::min<size_t>(kMaxPieces, std::max<uint64_t>(count, 1));
     std::vector<uint64_t> cut;  // first stripe of each piece, then count
-    size_t oi = 0, oo = 0, acc = 0;
+    size_t oi = 0, oo = 0, om = 0, acc = 0;
     for (uint64_t s = 0; s < count; s++) {
-        const scrs_stripe_desc& d = descs[s];
-        if (!d.in || !d.out) return set_err(err, SCRS_ERR_NULL_ARGUMENT, 0, s);
-        const size_t ib = (size_t)d.k * d.symbol_len;
+        const size_t ib = (size_t)descs[s].k * descs[s].symbol_len;
         if (cut.empty() || (acc * n_pieces >= in_bytes * cut.size() && cut.size() < n_pieces)) cut.push_back(s);
         acc += (ib + 15) & ~(size_t)15;
     }
@@ -445,19 +546,37 @@ extern "C" int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* b, const scrs_s
         if (first) {
             h2d_at.push_back(b->h2d.size());
             d2h_at.push_back(b->d2h.size());
+            b->missing_at.push_back(b->missing_copies.size());
         }
-        const uint64_t rows_out = d.op == SCRS_OP_ENCODE ? d.m : d.k;
-        const size_t ib = (size_t)d.k * d.symbol_len, ob = (size_t)rows_out * d.symbol_len;
+        const uint64_t L = d.symbol_len;
+        const size_t ib = (size_t)d.k * L, ob = (size_t)rows_out(d) * L;
         uint8_t* din = b->stage_in.as<uint8_t>() + oi;
         uint8_t* dout = b->stage_out.as<uint8_t>() + oo;
+        // device outputs land in the caller's buffer (repairs) or in the
+        // missing-row staging (decodes)
+        uint8_t* hout = d.op == SCRS_OP_DECODE ? b->h_missing.as<uint8_t>() + om : d.out;
         dev[s].in = din;
         dev[s].out = dout;
+        if (d.op == SCRS_OP_DECODE) {
+            const uint32_t k = d.k;
+            uint16_t row_of[256];
+            std::fill(row_of, row_of + std::min<uint32_t>(k, 256), kNoRow);
+            for (uint32_t q = 0; q < k; q++)
+                if (d.indices[q] < k && d.indices[q] < 256) row_of[d.indices[q]] = (uint16_t)q;
+            uint32_t t = 0;
+            for (uint32_t i = 0; i < k && i < 256; i++) {
+                if (row_of[i] != kNoRow)
+                    b->present_copies.push_back({d.in + (size_t)row_of[i] * L, d.out + (size_t)i * L, L});
+                else
+                    b->missing_copies.push_back({hout + (size_t)(t++) * L, d.out + (size_t)i * L, L});
+            }
+        }
         // merge with the previous copy of the same piece when both sides are
         // contiguous (the stripe's own copy is kept in case the driver refuses
         // a merged copy whose host side spans two allocations)
         const uint32_t part = (uint32_t)b->h2d_parts.size();
         b->h2d_parts.push_back({d.in, din, ib, part, part + 1, false});
-        b->d2h_parts.push_back({dout, d.out, ob, part, part + 1, false});
+        b->d2h_parts.push_back({dout, hout, ob, part, part + 1, false});
         if (!first && (const uint8_t*)b->h2d.back().src + b->h2d.back().bytes == d.in &&
             (uint8_t*)b->h2d.back().dst + b->h2d.back().bytes == din) {
             b->h2d.back().bytes += ib;
@@ -465,21 +584,29 @@ extern "C" int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* b, const scrs_s
         } else {
             b->h2d.push_back({d.in, din, ib, part, part + 1, false});
         }
-        if (!first && (const uint8_t*)b->d2h.back().src + b->d2h.back().bytes == dout &&
-            (uint8_t*)b->d2h.back().dst + b->d2h.back().bytes == d.out) {
-            b->d2h.back().bytes += ob;
-            b->d2h.back().part_hi = part + 1;
-        } else {
-            b->d2h.push_back({dout, d.out, ob, part, part + 1, false});
+        if (ob) {
+            const bool joins = b->d2h.size() > d2h_at.back() &&
+                               (const uint8_t*)b->d2h.back().src + b->d2h.back().bytes == dout &&
+                               (uint8_t*)b->d2h.back().dst + b->d2h.back().bytes == hout;
+            if (joins) {
+                b->d2h.back().bytes += ob;
+                b->d2h.back().part_hi = part + 1;
+            } else {
+                b->d2h.push_back({dout, hout, ob, part, part + 1, false});
+            }
         }
         oi += (ib + 15) & ~(size_t)15;
         oo += (ob + 15) & ~(size_t)15;
+        if (d.op == SCRS_OP_DECODE) om += (ob + 15) & ~(size_t)15;
         if (s + 1 == cut[piece + 1]) piece++;
     }
+    b->missing_at.push_back(b->missing_copies.size());
     const bool jit = b->jit;  // pieces are stripe ranges: keep the items in stripe order
     b->jit = false;
+    b->compact_decode = true;
     int32_t r = scrs_stripe_batch_set(b, dev.data(), count, err);
     b->jit = jit;
+    b->compact_decode = false;
     if (r) return r;
     b->pieces.clear();
     for (size_t q = 0; q + 1 < cut.size(); q++) {
@@ -497,10 +624,17 @@ extern "C" int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* b, const scrs_s
     }
     if (!b->s_in) SCRS_CUDA(cudaStreamCreateWithFlags(&b->s_in, cudaStreamNonBlocking));
     if (!b->s_out) SCRS_CUDA(cudaStreamCreateWithFlags(&b->s_out, cudaStreamNonBlocking));
-    while (b->events.size() < 2 + 2 * kMaxPieces) {
+    while (b->events.size() < 2 + 3 * kMaxPieces) {
         cudaEvent_t e;
         SCRS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         b->events.push_back(e);
+    }
+    if (!b->pool) {
+        b->pool.reset(new (std::nothrow) HostPool());
+        if (!b->pool) return set_err(err, SCRS_ERR_OUT_OF_MEMORY, sizeof(HostPool));
+        const unsigned hw = std::thread::hardware_concurrency();
+        b->pool->start((int)std::max(1u, std::min(8u, hw ? hw / 2 : 1u)));
+        if (b->pool->size() == 0) return set_err(err, SCRS_ERR_OUT_OF_MEMORY, sizeof(std::thread));
     }
     b->host_mode = true;
     return set_err(err, SCRS_OK);
@@ -611,7 +745,45 @@ int32_t enqueue_batch(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
     return SCRS_OK;
 }
 
-// Host-buffer run: copies and compute of consecutive pieces overlap (see top).
+// The host side of a host-buffer run's decode stripes, on the worker
+// threads: first every present row (caller's input row -> output row), then
+// piece by piece, once the piece's device->host copies are done (its event,
+// or nothing to wait for when `pieces_done`), the missing rows from the
+// staging.  Each worker takes a contiguous share of each list.
+int32_t host_copies(scrs_stripe_batch* b, bool pieces_done, scrs_error* err) {
+    if (b->present_copies.empty() && b->missing_copies.empty()) return SCRS_OK;
+    std::atomic<int> failed{0};
+    const int W = b->pool->size();
+    const std::function<void(int)> work = [&](int w) {
+        auto share = [&](size_t lo, size_t hi, int part) {
+            const size_t n = hi - lo;
+            return std::make_pair(lo + n * (size_t)part / (size_t)W, lo + n * (size_t)(part + 1) / (size_t)W);
+        };
+        const auto pr = share(0, b->present_copies.size(), w);
+        for (size_t i = pr.first; i < pr.second; i++)
+            memcpy(b->present_copies[i].dst, b->present_copies[i].src, b->present_copies[i].bytes);
+        for (size_t q = 0; q + 1 < b->missing_at.size(); q++) {
+            const auto mr = share(b->missing_at[q], b->missing_at[q + 1], w);
+            if (mr.first == mr.second) continue;
+            if (!pieces_done) {
+                const cudaError_t e = cudaEventSynchronize(b->events[2 + 2 * kMaxPieces + q]);
+                if (e != cudaSuccess) {
+                    failed.store((int)e);
+                    return;
+                }
+            }
+            for (size_t i = mr.first; i < mr.second; i++)
+                memcpy(b->missing_copies[i].dst, b->missing_copies[i].src, b->missing_copies[i].bytes);
+        }
+    };
+    b->pool->run(work);
+    if (failed.load()) return set_err(err, SCRS_ERR_CUDA, (uint64_t)failed.load(), __LINE__);
+    return SCRS_OK;
+}
+
+// Host-buffer run: copies and compute of consecutive pieces overlap (see
+// top).  Returns once the outputs are in the caller's buffers (the host
+// copies of the decode stripes' rows are part of the run).
 int32_t run_host(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
     cudaEvent_t ev_start = b->events[0], ev_end = b->events[1];
     SCRS_CUDA(cudaEventRecord(ev_start, st));
@@ -646,9 +818,12 @@ int32_t run_host(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
             int32_t r = issue_copy(b->d2h[i], b->d2h_parts, cudaMemcpyDeviceToHost, b->s_out, err);
             if (r) return r;
         }
+        SCRS_CUDA(cudaEventRecord(b->events[2 + 2 * kMaxPieces + q], b->s_out));
     }
     SCRS_CUDA(cudaEventRecord(ev_end, b->s_out));
     SCRS_CUDA(cudaStreamWaitEvent(st, ev_end, 0));
+    int32_t r = host_copies(b, false, err);
+    if (r) return r;
     return ran_on(b, st, err);
 }
 
@@ -710,7 +885,8 @@ extern "C" int32_t scrs_stripe_batch_run_plain(scrs_stripe_batch* b, void* strea
     b->last_launches = 0;
     size_t pi = 0;
     for (const MxkTask& T : b->tasks) {
-        if (T.pass_rows && T.n_out && pi < b->plans.size()) {  // decode stripe with erasures
+        // decode stripes carry row lists (encodes none); with erasures they have a plan
+        if (T.in_rows && T.n_out && pi < b->plans.size()) {
             SCRS_CUDA(launch_cauchy_plan_single(b->plans[pi++], 0, st));
             b->last_launches++;
         }
@@ -719,6 +895,11 @@ extern "C" int32_t scrs_stripe_batch_run_plain(scrs_stripe_batch* b, void* strea
     }
     r0 = copy_out(b, st, err);
     if (r0) return r0;
+    if (b->host_mode) {  // the decode stripes' rows on the host, after the copies back
+        SCRS_CUDA(cudaStreamSynchronize(st));
+        r0 = host_copies(b, true, err);
+        if (r0) return r0;
+    }
     return ran_on(b, st, err);
 }
 

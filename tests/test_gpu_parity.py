@@ -317,7 +317,10 @@ def test_stripe_batch_matches_oracle(gpu, oracle):
 
 def test_stripe_batch_host_buffers_pipelined(gpu, oracle):
     """Host-buffer batches run in up to 16 pieces whose copies overlap the
-    compute; results must equal the oracle's, run after run."""
+    compute; a decode stripe's present rows are copied on the host and only
+    its missing rows come back from the device.  Results must equal the
+    oracle's, run after run, pipelined and one launch per stripe, with decode
+    stripes that lost no data symbol among them."""
     torch = pytest.importorskip("torch")
     from scrs_b200.batch import OP_DECODE, OP_ENCODE, StripeBatch
 
@@ -349,14 +352,18 @@ def test_stripe_batch_host_buffers_pipelined(gpu, oracle):
     b = StripeBatch(gpu.lib, n)
     b.set_arrays(np.array(ops), np.array(engines), np.array(ks), np.array(ms), np.array(Ls),
                  np.array(ins, dtype=np.uint64), np.array(outs, dtype=np.uint64), indices=indices, host=True)
-    for _ in range(2):
+    assert any(s[0] == OP_DECODE and not any(i >= s[2] for i in indices[q, :s[2]]) for q, s in enumerate(specs))
+    for mode in ("pipelined", "pipelined", "plain"):
         for _, h_out in keep:
             h_out.zero_()
-        b.run()
+        if mode == "plain":
+            b.run_plain()
+        else:
+            b.run()
         torch.cuda.synchronize()
         b.check()
         for (_, h_out), exp in zip(keep, expect):
-            assert np.array_equal(h_out.numpy(), exp)
+            assert np.array_equal(h_out.numpy(), exp), mode
 
 
 @pytest.mark.parametrize("engine,k,m,L", [(Engine.GOOD_CAUCHY, 10, 4, 4096), (Engine.STANDARD_CAUCHY, 6, 3, 100),
