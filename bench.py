@@ -930,8 +930,8 @@ def extra_afft(torch, api, cpu=None):
              "decode_2_erasures_GBps": round(k * La / t_few / 1e6, 2),
              "encode_p50_ms": e50, "encode_p99_ms": e99, "decode_p50_ms": d50, "decode_p99_ms": d99,
              "decode_2_erasures_p50_ms": f50, "decode_2_erasures_p99_ms": f99,
-             "roofline": {"encode": roofline_of((k + m) * La, t_enc, "butterfly passes (afft_pass_kernel) + "
-                                                                     "slicing; latency-bound, see ncu summary"),
+             "roofline": {"encode": roofline_of((k + m) * La, t_enc, "butterfly passes (afft_tile_kernel), "
+                                                                     "slicing and unslicing fused into the first and last pass"),
                           "decode": roofline_of(2 * k * La, t_dec, "locator + transforms + derivative"),
                           "ncu_summary": "profiles/afft_tower_gf16_launches.md"}}
         if cpu is not None:

@@ -21,8 +21,6 @@ namespace scrs {
 namespace {
 
 constexpr uint32_t kMult = 65535u;  // multiplicative group order (afft/decoder.rs:580)
-constexpr int kPassThreads = 256;
-constexpr int kTileBytes = 64 * 1024;
 constexpr uint32_t kTargetedMax = 5;  // TARGETED_MAX_MISSING (afft/decoder.rs:578)
 
 // ---- GF(2^16) log/exp tables in device memory (afft/decoder.rs:587-598) --------
@@ -252,35 +250,6 @@ __device__ __forceinline__ void store_planes(uint8_t* p, const uint32_t (&w)[16]
         reinterpret_cast<uint4*>(p)[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
 }
 
-// work[i] = planes(values[i] * payload_i) for known i < n_rows_src, else 0
-// (the product evaluations of F*L, decoder.rs:320-333).  known == nullptr:
-// every row is known; values == nullptr: the rows are sliced unscaled.
-__global__ void __launch_bounds__(128) scale_in_kernel(const uint8_t* payloads, uint64_t L, uint32_t G,
-                                                       const uint8_t* known, const uint16_t* values,
-                                                       uint32_t ts, uint8_t* work, const uint16_t* row_map) {
-    const uint64_t total = (uint64_t)ts * G;
-    for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < total;
-         x += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t row = (uint32_t)(x / G), g = (uint32_t)(x % G);
-        uint32_t acc[16];
-#pragma unroll
-        for (int t = 0; t < 16; t++) acc[t] = 0;
-        if (!known || known[row]) {
-            uint32_t w[16];
-            const uint64_t src = row_map ? row_map[row] : row;
-            load_group_bytes(payloads + src * L, g, L, w);
-            bitslice16(w);
-            if (values) {
-                mul16<false>(values[row], acc, w);
-            } else {
-#pragma unroll
-                for (int t = 0; t < 16; t++) acc[t] = w[t];
-            }
-        }
-        store_planes(work + ((uint64_t)row * G + g) * 64, acc);
-    }
-}
-
 // Novel-basis formal derivative in gather form (transform.rs:188-213):
 // out[j] = sum over bits b with j_b = 0 of df[b] * in[j | 2^b].
 struct DerivFactors {
@@ -306,35 +275,6 @@ __global__ void __launch_bounds__(128) derivative_kernel(const uint8_t* in, uint
     }
 }
 
-// out row dst[t] = bytes(inv(derivs[src[t]]) * work[src[t]]) (decoder.rs:348-356);
-// derivs == nullptr: the rows are unsliced unscaled.
-__global__ void __launch_bounds__(128) scale_out_kernel(const uint8_t* work, uint32_t G, uint64_t L,
-                                                        const uint16_t* rows_src, const uint16_t* rows_dst,
-                                                        uint32_t count, const uint16_t* derivs,
-                                                        const uint16_t* log16, const uint16_t* exp16,
-                                                        uint8_t* out) {
-    const uint64_t total = (uint64_t)count * G;
-    for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < total;
-         x += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t t = (uint32_t)(x / G), g = (uint32_t)(x % G);
-        const uint32_t src = rows_src[t];
-        uint32_t w[16], acc[16];
-        load_planes(work + ((uint64_t)src * G + g) * 64, w);
-        if (derivs) {
-            const uint16_t d = derivs[src];
-            const uint16_t f = d ? exp16[(kMult - log16[d]) % kMult] : 0;
-#pragma unroll
-            for (int q = 0; q < 16; q++) acc[q] = 0;
-            mul16<false>(f, acc, w);
-        } else {
-#pragma unroll
-            for (int q = 0; q < 16; q++) acc[q] = w[q];
-        }
-        bitslice16(acc);
-        store_group_bytes(out + (uint64_t)rows_dst[t] * L, g, L, acc);
-    }
-}
-
 // dst row rows[t] = src row (row_map ? row_map[rows[t]] : rows[t]), L bytes
 // each, in units of `unit` bytes (16 when both bases are 16-byte aligned and
 // L is a multiple of 16, else 1).
@@ -353,80 +293,219 @@ __global__ void copy_rows_kernel(const uint8_t* src, uint8_t* dst, uint64_t L, c
     }
 }
 
-// Several butterfly levels of one transform on a shared-memory tile
+// ---- transform passes ---------------------------------------------------------
+// Several butterfly levels of a transform of 2^D rows on a shared-memory tile
 // (transform.rs:301-333 forward_node / inverse_node, flattened by level).
-// Rows p and p + 2^(D-1-l) pair at level l; the node factor is
-// factors[root*2^l + (p >> (D-l))].  A tile holds the 2^c rows that differ
-// only in the c index bits of levels [l0, l0+c), for gt groups of columns.
-__global__ void __launch_bounds__(kPassThreads) afft_pass_kernel(uint8_t* work, uint32_t G, int D, uint32_t root,
-                                                                 int l0, int c, int forward,
-                                                                 const uint16_t* factors, uint32_t gt) {
+// Rows p and p + 2^(D-1-l) pair at level l with node factor
+// factors[root*2^l + (p >> (D-l))]: rows that agree in their top l bits share
+// it.  A tile holds the rows that differ only in the c "level bits"
+// [D-l0-c, D-l0) of the pass's levels [l0, l0+c) and in the e lowest row
+// bits, for gn <= gt column groups.  The low bits lie below every level bit,
+// so rows that differ only in them share every factor of the pass: lanes run
+// over (group, low bits) first, and a level whose factor blocks of
+// gn * 2^(e + b) butterflies (b: the level's pair bit among the level bits)
+// are whole warps sends each warp through one factor.  Elsewhere (the
+// deepest levels of a transform, which have no lower bits) the lanes of a
+// warp are served factor by factor, each group with the uniform jump table,
+// so the kernel holds a single copy of the multiply code.
+//
+// A pass runs one or two phases on the same tile (root, direction): the
+// encode of a power-of-two k runs its inverse left half-transform's top
+// levels and its forward right half-transform's top levels in one launch.
+// With `slice` (the first pass of a transform) the tile is loaded from byte
+// rows, bit-sliced and scaled on the way in; with `unslice` (the last pass)
+// the output rows are scaled, converted back to bytes and stored to the
+// caller's output instead of the work array (see PassIo).
+constexpr int kTileThreads = 256;
+constexpr uint32_t kTileElems = 1024;  // (row, group) elements of 64 bytes: 64 KiB
+constexpr uint32_t kTileNominal = 512; // elements the deepest pass's tile aims at (32 KiB)
+
+struct PassPhases {
+    uint32_t root[2];
+    int32_t forward[2];
+    int32_t n;
+};
+
+struct PassIo {
+    // slice (first pass): tile row r <- the bit-sliced bytes of payload row
+    // (row_map ? row_map[r] : r) of src, times in_scale[r] when given, for
+    // r < n_src that are known (known == nullptr: all); zero otherwise
+    const uint8_t* src;
+    const uint8_t* known;
+    const uint16_t* row_map;
+    const uint16_t* in_scale;
+    uint32_t n_src;
+    // unslice (last pass): rows r in [out_lo, out_hi) that are not known,
+    // divided by out_derivs[r] when given, as bytes to dst row r - out_lo
+    uint32_t out_lo, out_hi;
+    uint8_t* dst;
+    const uint16_t* out_derivs;
+    const uint16_t* log16;
+    const uint16_t* exp16;
+    uint64_t L;
+};
+
+// acc ^= f * x for every lane of the calling warp (all 32 lanes call it
+// together; a lane with nothing to multiply passes f = 0), each lane with its
+// own factor: the warp's distinct factors are served one at a time, every
+// group through the uniform jump table (brx.idx.uni is valid there: all
+// active lanes share the index).  A warp whose lanes share one factor makes
+// one pass.
+__device__ __forceinline__ void mul16_lanes(uint32_t f, uint32_t (&acc)[16], const uint32_t (&x)[16]) {
+    unsigned left = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    while (left) {
+        const uint32_t fl = __shfl_sync(0xFFFFFFFFu, f, __ffs(left) - 1);
+        const bool mine = ((left >> lane) & 1u) && f == fl;
+        const unsigned grp = __ballot_sync(0xFFFFFFFFu, mine);
+        if (mine && fl) mul16<true>(fl, acc, x);
+        left &= ~grp;
+    }
+}
+
+__global__ void __launch_bounds__(kTileThreads) afft_tile_kernel(uint8_t* work, uint32_t G, int D, int l0, int c,
+                                                                int e, uint32_t gt, PassPhases ph,
+                                                                const uint16_t* factors, PassIo io, int slice,
+                                                                int unslice) {
     extern __shared__ __align__(16) uint8_t tile[];
     const uint32_t col_tiles = (G + gt - 1) / gt;
-    const uint32_t low_bits = (uint32_t)(D - l0 - c);
+    const int low_bits = D - l0 - c;   // row bits below the level bits
+    const int mid_bits = low_bits - e; // of which the tile fixes these
     const uint32_t tid = threadIdx.x;
-    const uint32_t rows_in_tile = 1u << c;
-    // tile id -> (high index, low index, column tile)
-    uint32_t tidx = blockIdx.x;
-    const uint32_t ct = tidx % col_tiles;
-    tidx /= col_tiles;
-    const uint32_t lo = tidx & ((1u << low_bits) - 1u);
-    const uint32_t hi = tidx >> low_bits;
+    uint32_t t = blockIdx.x;
+    const uint32_t ct = t % col_tiles;
+    t /= col_tiles;
+    const uint32_t mid = t & ((1u << mid_bits) - 1u);
+    const uint32_t hi = t >> mid_bits;
     const uint32_t g0 = ct * gt;
     const uint32_t gn = min(gt, G - g0);
-    auto row_of = [&](uint32_t i) { return (hi << (D - l0)) | (i << low_bits) | lo; };
-    // load: element (i, g, q) = 16 bytes, smem at ((i*4 + q)*gt + g)*16; the
-    // copies are asynchronous, so every thread has all of its loads in flight
-    const uint32_t pieces = rows_in_tile * gn * 4;
-    for (uint32_t x = tid; x < pieces; x += blockDim.x) {
-        const uint32_t q = x & 3, g = (x >> 2) % gn, i = (x >> 2) / gn;
-        cp_async_16(tile + ((size_t)(i * 4 + q) * gt + g) * 16,
-                    work + ((uint64_t)row_of(i) * G + g0 + g) * 64 + 16 * q);
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    const uint32_t pairs = rows_in_tile / 2;
-    for (int s = 0; s < c; s++) {
-        const int lam = forward ? s : c - 1 - s;  // tile-local level
-        const int l = l0 + lam;
-        const uint32_t b = (uint32_t)(c - 1 - lam);  // tile index bit of this level
-        for (uint32_t x = tid; x < pairs * gn; x += blockDim.x) {
-            const uint32_t g = x % gn, pi = x / gn;
-            const uint32_t ilo = ((pi >> b) << (b + 1)) | (pi & ((1u << b) - 1u));
-            const uint32_t ihi = ilo | (1u << b);
-            const uint32_t node = (root << l) + (row_of(ilo) >> (D - l));
-            const uint32_t f = factors[node];
-            uint32_t wl[16], wh[16];
+    const uint32_t rows = 1u << (c + e);
+    const uint32_t low_mask = (1u << e) - 1u;
+    // tile row i = (level bits << e) | low bits
+    auto row_of = [&](uint32_t i) {
+        return (hi << (D - l0)) | ((i >> e) << low_bits) | (mid << e) | (i & low_mask);
+    };
+    auto piece = [&](uint32_t i, uint32_t q, uint32_t g) { return tile + ((size_t)(i * 4 + q) * gt + g) * 16; };
+    // Loops that multiply run whole warps: every lane of a warp takes the same
+    // iterations (x0 is the warp's first element), lanes past the end with
+    // nothing to do, so that mul16_lanes always has all 32 lanes.
+    const uint32_t lane = tid & 31u;
+    if (slice) {
+        for (uint32_t x0 = tid - lane; x0 < rows * gn; x0 += blockDim.x) {
+            const uint32_t x = x0 + lane;
+            const bool valid = x < rows * gn;
+            const uint32_t g = valid ? x % gn : 0u, i = valid ? x / gn : 0u;
+            const uint32_t r = row_of(i);
+            const bool have = valid && r < io.n_src && (!io.known || io.known[r]);
+            uint32_t w[16], acc[16];
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                uint4 a = *reinterpret_cast<const uint4*>(tile + ((size_t)(ilo * 4 + q) * gt + g) * 16);
-                uint4 h = *reinterpret_cast<const uint4*>(tile + ((size_t)(ihi * 4 + q) * gt + g) * 16);
-                wl[4 * q] = a.x, wl[4 * q + 1] = a.y, wl[4 * q + 2] = a.z, wl[4 * q + 3] = a.w;
-                wh[4 * q] = h.x, wh[4 * q + 1] = h.y, wh[4 * q + 2] = h.z, wh[4 * q + 3] = h.w;
+            for (int q = 0; q < 16; q++) acc[q] = 0, w[q] = 0;
+            if (have) {
+                load_group_bytes(io.src + (uint64_t)(io.row_map ? io.row_map[r] : r) * io.L, g0 + g, io.L, w);
+                bitslice16(w);
+                if (!io.in_scale) {
+#pragma unroll
+                    for (int q = 0; q < 16; q++) acc[q] = w[q];
+                }
             }
-            if (forward) {  // low ^= f*high; high ^= low
-                if (f) mul16<false>(f, wl, wh);
+            if (io.in_scale) mul16_lanes(have ? io.in_scale[r] : 0u, acc, w);
+            if (!valid) continue;
 #pragma unroll
-                for (int q = 0; q < 16; q++) wh[q] ^= wl[q];
-            } else {  // high ^= low; low ^= f*high
-#pragma unroll
-                for (int q = 0; q < 16; q++) wh[q] ^= wl[q];
-                if (f) mul16<false>(f, wl, wh);
-            }
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                *reinterpret_cast<uint4*>(tile + ((size_t)(ilo * 4 + q) * gt + g) * 16) =
-                    make_uint4(wl[4 * q], wl[4 * q + 1], wl[4 * q + 2], wl[4 * q + 3]);
-                *reinterpret_cast<uint4*>(tile + ((size_t)(ihi * 4 + q) * gt + g) * 16) =
-                    make_uint4(wh[4 * q], wh[4 * q + 1], wh[4 * q + 2], wh[4 * q + 3]);
-            }
+            for (int q = 0; q < 4; q++)
+                *reinterpret_cast<uint4*>(piece(i, q, g)) =
+                    make_uint4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
         }
-        __syncthreads();
+    } else {
+        // the copies are asynchronous, so every thread has all of its loads in flight
+        for (uint32_t x = tid; x < rows * gn * 4; x += blockDim.x) {
+            const uint32_t q = x & 3, g = (x >> 2) % gn, i = (x >> 2) / gn;
+            cp_async_16(piece(i, q, g), work + ((uint64_t)row_of(i) * G + g0 + g) * 64 + 16 * q);
+        }
+        cp_async_wait_all();
     }
-    for (uint32_t x = tid; x < pieces; x += blockDim.x) {
+    __syncthreads();
+    const uint32_t items = (rows / 2) * gn;
+    for (int p = 0; p < ph.n; p++) {
+        const uint32_t root = ph.root[p];
+        const bool fwd = ph.forward[p] != 0;
+        for (int s = 0; s < c; s++) {
+            const int lam = fwd ? s : c - 1 - s;  // tile-local level
+            const int l = l0 + lam;
+            const int b = c - 1 - lam;            // pair bit among the level bits
+            for (uint32_t x0 = tid - lane; x0 < items; x0 += blockDim.x) {
+                const uint32_t x = x0 + lane;
+                const bool valid = x < items;
+                const uint32_t g = valid ? x % gn : 0u;
+                uint32_t r = valid ? x / gn : 0u;
+                const uint32_t low = r & low_mask;
+                r >>= e;
+                const uint32_t lev_lo = ((r >> b) << (b + 1)) | (r & ((1u << b) - 1u));
+                const uint32_t ilo = (lev_lo << e) | low, ihi = ilo | (1u << (b + e));
+                const uint32_t f = valid ? factors[(root << l) + (row_of(ilo) >> (D - l))] : 0u;
+                uint32_t wl[16], wh[16];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const uint4 a = *reinterpret_cast<const uint4*>(piece(ilo, q, g));
+                    const uint4 h = *reinterpret_cast<const uint4*>(piece(ihi, q, g));
+                    wl[4 * q] = a.x, wl[4 * q + 1] = a.y, wl[4 * q + 2] = a.z, wl[4 * q + 3] = a.w;
+                    wh[4 * q] = h.x, wh[4 * q + 1] = h.y, wh[4 * q + 2] = h.z, wh[4 * q + 3] = h.w;
+                }
+                // forward: low ^= f*high, high ^= low;  inverse: high ^= low, low ^= f*high
+                if (!fwd) {
+#pragma unroll
+                    for (int q = 0; q < 16; q++) wh[q] ^= wl[q];
+                }
+                mul16_lanes(f, wl, wh);
+                if (fwd) {
+#pragma unroll
+                    for (int q = 0; q < 16; q++) wh[q] ^= wl[q];
+                }
+                if (!valid) continue;
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    *reinterpret_cast<uint4*>(piece(ilo, q, g)) =
+                        make_uint4(wl[4 * q], wl[4 * q + 1], wl[4 * q + 2], wl[4 * q + 3]);
+                    *reinterpret_cast<uint4*>(piece(ihi, q, g)) =
+                        make_uint4(wh[4 * q], wh[4 * q + 1], wh[4 * q + 2], wh[4 * q + 3]);
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (unslice) {
+        for (uint32_t x0 = tid - lane; x0 < rows * gn; x0 += blockDim.x) {
+            const uint32_t x = x0 + lane;
+            const bool valid = x < rows * gn;
+            const uint32_t g = valid ? x % gn : 0u, i = valid ? x / gn : 0u;
+            const uint32_t r = row_of(i);
+            const bool out = valid && r >= io.out_lo && r < io.out_hi && !(io.known && io.known[r]);
+            uint32_t w[16], acc[16];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const uint4 v = *reinterpret_cast<const uint4*>(piece(i, q, g));
+                w[4 * q] = v.x, w[4 * q + 1] = v.y, w[4 * q + 2] = v.z, w[4 * q + 3] = v.w;
+            }
+            if (io.out_derivs) {
+                // 1 / L'(r) through the log tables (decoder.rs:348-356)
+                const uint32_t d = out ? io.out_derivs[r] : 0u;
+                const uint32_t f = d ? io.exp16[(kMult - io.log16[d]) % kMult] : 0u;
+#pragma unroll
+                for (int q = 0; q < 16; q++) acc[q] = 0;
+                mul16_lanes(f, acc, w);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 16; q++) acc[q] = w[q];
+            }
+            if (!out) continue;
+            bitslice16(acc);
+            store_group_bytes(io.dst + (uint64_t)(r - io.out_lo) * io.L, g0 + g, io.L, acc);
+        }
+        return;
+    }
+    for (uint32_t x = tid; x < rows * gn * 4; x += blockDim.x) {
         const uint32_t q = x & 3, g = (x >> 2) % gn, i = (x >> 2) / gn;
         *reinterpret_cast<uint4*>(work + ((uint64_t)row_of(i) * G + g0 + g) * 64 + 16 * q) =
-            *reinterpret_cast<const uint4*>(tile + ((size_t)(i * 4 + q) * gt + g) * 16);
+            *reinterpret_cast<const uint4*>(piece(i, q, g));
     }
 }
 
@@ -435,43 +514,123 @@ int grid_for(uint64_t items, int threads) {
     return (int)std::max<uint64_t>(1, std::min<uint64_t>(g, 148ull * 32));
 }
 
-// Full transform of 2^D bit-sliced rows (heap root 1), forward or inverse.
-// root: heap index of the transform's root node (1: the whole transform of
-// 2^D rows; 2 and 3: the halves below it, each of 2^D rows, D one less).
-cudaError_t run_transform(uint8_t* work, uint32_t G, int D, const uint16_t* factors, bool forward,
-                          cudaStream_t st, uint32_t root = 1) {
-    static std::atomic<uint64_t> attr{0};
-    cudaError_t ea = once_per_device(attr, [] {
-        return cudaFuncSetAttribute(afft_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileBytes);
-    });
-    if (ea != cudaSuccess) return ea;
-    // Column groups per tile: up to 8 of one row pair, so that the lanes of a
-    // warp (consecutive groups of a few pairs) mostly share the butterfly
-    // factor, and tiles stay small enough for two-level-count passes
-    // (k = m = 4096, L = 1024: 8 groups give 2 passes of 6-7 levels, 16 gave 3).
-    const uint32_t gt = std::min<uint32_t>(G, 8);
-    int cmax = 1;
-    while (cmax < D && ((size_t)2 << cmax) * gt * 64 <= (size_t)kTileBytes) cmax++;
-    const uint32_t col_tiles = (G + gt - 1) / gt;
-    // The fewest passes the tile size allows (a pass more costs more than the
-    // parallelism it adds), levels spread evenly over them.
-    const int n_pass = (D + cmax - 1) / cmax;
-    std::vector<std::pair<int, int>> passes;  // (l0, c) top-down
-    for (int q = 0, l0 = 0; q < n_pass; q++) {
-        const int c = D / n_pass + (q < D % n_pass ? 1 : 0);
-        passes.push_back({l0, c});
-        l0 += c;
+int log2_floor(uint32_t v) {
+    int r = 0;
+    while (v >>= 1) r++;
+    return r;
+}
+
+// Column groups per tile: a power of two, at most 16 (whole rows up to L = 1 KiB).
+uint32_t tile_groups(uint32_t G) {
+    uint32_t gt = 1;
+    while (gt * 2 <= std::min<uint32_t>(G, 16)) gt *= 2;
+    return gt;
+}
+
+struct PassPlan {
+    int l0, c, e;
+};
+
+// Passes of a transform of 2^D rows, top-down: the deepest pass has no row
+// bits below its levels (e = 0) and takes log2(kTileNominal / gt) levels;
+// the passes above it take the low bits a uniform factor per warp needs
+// (gt * 2^e >= 32) and at most log2(kTileElems / gt) - e levels each, as
+// few passes as that allows with the levels spread evenly.
+std::vector<PassPlan> plan_passes(int D, uint32_t gt) {
+    std::vector<PassPlan> out;
+    if (D <= 0) return out;
+    const int c_last = std::min(D, log2_floor(kTileNominal / gt));
+    const int rest = D - c_last;
+    if (rest > 0) {
+        const int e = std::max(0, 5 - log2_floor(gt));
+        const int c_max = std::max(1, log2_floor(kTileElems / gt) - e);
+        const int n = (rest + c_max - 1) / c_max;
+        for (int q = 0, l0 = 0; q < n; q++) {
+            const int c = rest / n + (q < rest % n ? 1 : 0);
+            out.push_back({l0, c, std::min(e, D - l0 - c)});
+            l0 += c;
+        }
     }
-    if (!forward) std::reverse(passes.begin(), passes.end());
-    for (auto& pc : passes) {
-        const int l0 = pc.first, c = pc.second;
-        const uint32_t tiles = (1u << (D - c)) * col_tiles;
-        const size_t smem = ((size_t)1 << c) * gt * 64;
-        // one butterfly per thread and level (a multiple of 32, at most kPassThreads)
-        const uint32_t bfly = (1u << (c - 1)) * gt;
-        const int threads = (int)std::min<uint32_t>(kPassThreads, std::max<uint32_t>(32, (bfly + 31) / 32 * 32));
-        afft_pass_kernel<<<tiles, threads, smem, st>>>(work, G, D, root, l0, c, forward ? 1 : 0, factors, gt);
-        cudaError_t e = cudaGetLastError();
+    out.push_back({rest, c_last, 0});
+    return out;
+}
+
+cudaError_t set_tile_attr() {
+    static std::atomic<uint64_t> attr{0};
+    return once_per_device(attr, [] {
+        return cudaFuncSetAttribute(afft_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(kTileElems * 64));
+    });
+}
+
+cudaError_t launch_pass(uint8_t* work, uint32_t G, int D, const PassPlan& P, uint32_t gt, const PassPhases& ph,
+                        const uint16_t* factors, const PassIo& io, int slice, int unslice, cudaStream_t st) {
+    const uint32_t col_tiles = (G + gt - 1) / gt;
+    const uint32_t tiles = (1u << (D - P.c - P.e)) * col_tiles;
+    const size_t smem = ((size_t)1 << (P.c + P.e)) * gt * 64;
+    afft_tile_kernel<<<tiles, kTileThreads, smem, st>>>(work, G, D, P.l0, P.c, P.e, gt, ph, factors, io, slice,
+                                                        unslice);
+    return cudaGetLastError();
+}
+
+// Full transform of 2^D bit-sliced rows (heap root `root`: 1 for the whole
+// transform; 2 and 3 for the halves below it, each of 2^D rows, D one less),
+// forward (top-down) or inverse (bottom-up).  With io.src the first pass
+// slices the rows in from bytes (see PassIo); with io.dst the last pass
+// writes its output rows as bytes instead of back to the work array.
+cudaError_t run_transform(uint8_t* work, uint32_t G, int D, const uint16_t* factors, bool forward,
+                          cudaStream_t st, uint32_t root = 1, const PassIo& io = PassIo{}) {
+    cudaError_t e = set_tile_attr();
+    if (e != cudaSuccess) return e;
+    const uint32_t gt = tile_groups(G);
+    std::vector<PassPlan> plan = plan_passes(D, gt);
+    if (!forward) std::reverse(plan.begin(), plan.end());
+    const PassPhases ph{{root, 0}, {forward ? 1 : 0, 0}, 1};
+    for (size_t q = 0; q < plan.size(); q++) {
+        e = launch_pass(work, G, D, plan[q], gt, ph, factors, io, q == 0 && io.src, q + 1 == plan.size() && io.dst,
+                        st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// Encode of a power-of-two k (ts = 2k, m <= k): the k data rows bit-sliced
+// into the work array, the inverse transform over them as the left half
+// (heap root 2), the forward transform of the result as the right half
+// (root 3), its first m rows unsliced into the repairs.  The inverse's top
+// pass and the forward's top pass share one launch; the first pass slices
+// the data on the way in, the last one unslices the repairs on the way out.
+cudaError_t run_encode_halves(uint8_t* work, uint32_t G, int D, const uint16_t* factors, const uint8_t* data,
+                              uint32_t k, uint32_t m, uint64_t L, uint8_t* repairs, cudaStream_t st) {
+    cudaError_t e = set_tile_attr();
+    if (e != cudaSuccess) return e;
+    const uint32_t gt = tile_groups(G);
+    const std::vector<PassPlan> plan = plan_passes(D, gt);  // top-down
+    const size_t np = plan.size();
+    PassIo io{};
+    io.src = data;
+    io.n_src = k;
+    io.dst = repairs;
+    io.out_lo = 0;
+    io.out_hi = m;
+    io.L = L;
+    if (np == 0) {  // k = 1: no levels; the one data row is the repair
+        const PassPhases none{{0, 0}, {0, 0}, 0};
+        return launch_pass(work, G, 0, PassPlan{0, 0, 0}, gt, none, factors, io, 1, 1, st);
+    }
+    // inverse, bottom-up: plan[np-1] .. plan[1]; then plan[0] inverse + forward;
+    // then forward top-down: plan[1] .. plan[np-1]
+    for (size_t q = np; q-- > 1;) {
+        const PassPhases inv{{2, 0}, {0, 0}, 1};
+        e = launch_pass(work, G, D, plan[q], gt, inv, factors, io, q == np - 1, 0, st);
+        if (e != cudaSuccess) return e;
+    }
+    const PassPhases both{{2, 3}, {0, 1}, 2};
+    e = launch_pass(work, G, D, plan[0], gt, both, factors, io, np == 1, np == 1, st);
+    if (e != cudaSuccess) return e;
+    for (size_t q = 1; q < np; q++) {
+        const PassPhases fw{{3, 0}, {1, 0}, 1};
+        e = launch_pass(work, G, D, plan[q], gt, fw, factors, io, 0, q == np - 1, st);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -754,34 +913,35 @@ int32_t AfftCodec::encode(const uint8_t* d_data, uint8_t* d_repairs, AfftWorkspa
         // inverse of the data: two transforms of k points, no locator, no
         // derivative (the reference encoder is this IFFT-then-forward form,
         // afft/encoder.rs:150-250).
-        scale_in_kernel<<<grid_for(k * G, 128), 128, 0, st>>>(d_data, L, G, nullptr, nullptr, (uint32_t)k,
-                                                              ws.work0.as<uint8_t>(), nullptr);
-        SCRS_CUDA(cudaGetLastError());
-        SCRS_CUDA(run_transform(ws.work0.as<uint8_t>(), G, (int)log_ts - 1, factors.as<uint16_t>(), false, st, 2));
-        SCRS_CUDA(run_transform(ws.work0.as<uint8_t>(), G, (int)log_ts - 1, factors.as<uint16_t>(), true, st, 3));
-        scale_out_kernel<<<grid_for(m * G, 128), 128, 0, st>>>(ws.work0.as<uint8_t>(), G, L,
-                                                               ws.rows.as<uint16_t>() + m, ws.rows.as<uint16_t>() + m,
-                                                               (uint32_t)m, nullptr, nullptr, nullptr, d_repairs);
-        SCRS_CUDA(cudaGetLastError());
+        SCRS_CUDA(run_encode_halves(ws.work0.as<uint8_t>(), G, (int)log_ts - 1, factors.as<uint16_t>(), d_data,
+                                    (uint32_t)k, (uint32_t)m, L, d_repairs, st));
         return SCRS_OK;
     }
+    // general k: the erasure-decode form with E = [k, ts) (see afft_engine.h)
     const uint16_t *lg, *ex;
     SCRS_CUDA(log16_tables(&lg, &ex));
-    scale_in_kernel<<<grid_for(ts * G, 128), 128, 0, st>>>(d_data, L, G, ws.known.as<uint8_t>(),
-                                                           enc_values.as<uint16_t>(), (uint32_t)ts,
-                                                           ws.work0.as<uint8_t>(), nullptr);
-    SCRS_CUDA(cudaGetLastError());
-    SCRS_CUDA(run_transform(ws.work0.as<uint8_t>(), G, (int)log_ts, factors.as<uint16_t>(), false, st));
+    PassIo in{};
+    in.src = d_data;
+    in.known = ws.known.as<uint8_t>();
+    in.in_scale = enc_values.as<uint16_t>();
+    in.n_src = (uint32_t)k;
+    in.L = L;
+    SCRS_CUDA(run_transform(ws.work0.as<uint8_t>(), G, (int)log_ts, factors.as<uint16_t>(), false, st, 1, in));
     DerivFactors df{};
     std::copy(deriv_factors, deriv_factors + 16, df.f);
     derivative_kernel<<<grid_for(ts * G, 128), 128, 0, st>>>(ws.work0.as<uint8_t>(), ws.work1.as<uint8_t>(),
                                                              (uint32_t)ts, G, (int)log_ts, df);
     SCRS_CUDA(cudaGetLastError());
-    SCRS_CUDA(run_transform(ws.work1.as<uint8_t>(), G, (int)log_ts, factors.as<uint16_t>(), true, st));
-    scale_out_kernel<<<grid_for(m * G, 128), 128, 0, st>>>(ws.work1.as<uint8_t>(), G, L, ws.rows.as<uint16_t>(),
-                                                           ws.rows.as<uint16_t>() + m, (uint32_t)m,
-                                                           enc_derivs.as<uint16_t>(), lg, ex, d_repairs);
-    SCRS_CUDA(cudaGetLastError());
+    PassIo out{};
+    out.known = ws.known.as<uint8_t>();
+    out.out_lo = (uint32_t)k;
+    out.out_hi = (uint32_t)(k + m);
+    out.dst = d_repairs;
+    out.out_derivs = enc_derivs.as<uint16_t>();
+    out.log16 = lg;
+    out.exp16 = ex;
+    out.L = L;
+    SCRS_CUDA(run_transform(ws.work1.as<uint8_t>(), G, (int)log_ts, factors.as<uint16_t>(), true, st, 1, out));
     return SCRS_OK;
 }
 
@@ -805,7 +965,6 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
             miss[nm++] = (uint16_t)d;
     }
     SCRS_CUDA(cudaMemcpyAsync(ws.rows.p, miss, (2 * k + 8) * 2, cudaMemcpyHostToDevice, st));
-    const uint16_t* d_miss = ws.rows.as<uint16_t>();
     const uint16_t* d_pres = ws.rows.as<uint16_t>() + k;
     const uint16_t* d_map = nullptr;
     if (row_map) {
@@ -840,20 +999,30 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
                                     ws.wht_b.as<uint32_t>(), ws.values.as<uint16_t>(), ws.derivs.as<uint16_t>(), st,
                                     err);
     if (r) return r;
-    scale_in_kernel<<<grid_for(ts * G, 128), 128, 0, st>>>(d_payloads, L, G, ws.known.as<uint8_t>(),
-                                                           ws.values.as<uint16_t>(), (uint32_t)ts,
-                                                           ws.work0.as<uint8_t>(), d_map);
-    SCRS_CUDA(cudaGetLastError());
-    SCRS_CUDA(run_transform(ws.work0.as<uint8_t>(), G, (int)log_ts, factors.as<uint16_t>(), false, st));
+    PassIo in{};
+    in.src = d_payloads;
+    in.known = ws.known.as<uint8_t>();
+    in.row_map = d_map;
+    in.in_scale = ws.values.as<uint16_t>();
+    in.n_src = (uint32_t)ts;
+    in.L = L;
+    SCRS_CUDA(run_transform(ws.work0.as<uint8_t>(), G, (int)log_ts, factors.as<uint16_t>(), false, st, 1, in));
     DerivFactors df{};
     std::copy(deriv_factors, deriv_factors + 16, df.f);
     derivative_kernel<<<grid_for(ts * G, 128), 128, 0, st>>>(ws.work0.as<uint8_t>(), ws.work1.as<uint8_t>(),
                                                              (uint32_t)ts, G, (int)log_ts, df);
     SCRS_CUDA(cudaGetLastError());
-    SCRS_CUDA(run_transform(ws.work1.as<uint8_t>(), G, (int)log_ts, factors.as<uint16_t>(), true, st));
-    scale_out_kernel<<<grid_for((uint64_t)nm * G, 128), 128, 0, st>>>(ws.work1.as<uint8_t>(), G, L, d_miss, d_miss,
-                                                                      nm, ws.derivs.as<uint16_t>(), lg, ex, d_out);
-    SCRS_CUDA(cudaGetLastError());
+    // the missing data rows: rows of [0, k) not known
+    PassIo out{};
+    out.known = ws.known.as<uint8_t>();
+    out.out_lo = 0;
+    out.out_hi = (uint32_t)k;
+    out.dst = d_out;
+    out.out_derivs = ws.derivs.as<uint16_t>();
+    out.log16 = lg;
+    out.exp16 = ex;
+    out.L = L;
+    SCRS_CUDA(run_transform(ws.work1.as<uint8_t>(), G, (int)log_ts, factors.as<uint16_t>(), true, st, 1, out));
     return SCRS_OK;
 }
 
