@@ -861,6 +861,9 @@ def extra_tower(torch, api, cpu=None):
            "encode_p50_ms": e50, "encode_p99_ms": e99, "decode_p50_ms": d50, "decode_p99_ms": d99,
            "roofline": {"encode": roofline_of((k + m) * Lt, t_enc, "32 feeds + one fold launch, per call"),
                         "decode": roofline_of(2 * k * Lt, t_dec, "32 pushes + plan + multiply-XOR, per call")}}
+    res["batched"] = tower_batched(torch, api, k, m, Lt, np.concatenate([r.cpu().numpy() for r in reps]),
+                                   data.cpu().numpy().reshape(-1))
+    ok &= res["batched"]["bit_exact"]
     if cpu is not None:
         h_data = data.cpu().numpy().reshape(-1)
         h_word = [w.cpu().numpy() for w in word]
@@ -873,6 +876,57 @@ def extra_tower(torch, api, cpu=None):
         ok &= legs["encode"]["bit_exact"] and legs["decode"]["bit_exact"]
     res["bit_exact"] = ok
     return res
+
+
+def tower_batched(torch, api, k, m, Lt, rep0, data0, n=128, seed=SEED + 22):
+    """The cfg2 geometry as stripes of one batch: n tower encodes and n tower
+    decodes (8 data symbols erased each, random arrival order) in one plan
+    launch + one persistent drain, replayed as a CUDA graph.  Stripe 0's
+    data is the per-call extra's, so its repairs are checked against the
+    incremental encoder's; every decode against its data."""
+    from scrs_b200.api import Engine
+    from scrs_b200.batch import OP_DECODE, OP_ENCODE, StripeBatch
+
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    data = torch.randint(0, 256, (n, k * Lt), dtype=torch.uint8, device="cuda", generator=gen)
+    data[0].copy_(torch.from_numpy(data0))
+    reps = torch.zeros((n, m * Lt), dtype=torch.uint8, device="cuda")
+    eng = int(Engine.TOWER)
+    b = StripeBatch(api.lib, 2 * n)
+    idx = np.arange(n, dtype=np.uint64)
+    b.set_arrays(np.full(n, OP_ENCODE), np.full(n, eng), np.full(n, k), np.full(n, m), np.full(n, Lt),
+                 data.data_ptr() + idx * (k * Lt), reps.data_ptr() + idx * (m * Lt))
+    b.run()
+    torch.cuda.synchronize()
+    ok = bool(np.array_equal(reps[0].cpu().numpy(), rep0))
+    rng = np.random.default_rng(seed)
+    recv = np.zeros((n, k), np.int64)
+    for s in range(n):
+        erased = set(rng.choice(k, 8, replace=False).tolist())
+        recv[s] = [i for i in rng.permutation(k + m).tolist() if i not in erased][:k]
+    word = torch.cat([data.view(n, k, Lt), reps.view(n, m, Lt)], dim=1)
+    received = word[torch.arange(n, device="cuda")[:, None], torch.from_numpy(recv).cuda()].reshape(n, k * Lt)
+    del word
+    out = torch.zeros((n, k * Lt), dtype=torch.uint8, device="cuda")
+    enc_out = torch.zeros_like(reps)
+    op = np.concatenate([np.full(n, OP_ENCODE), np.full(n, OP_DECODE)])
+    ins = np.concatenate([data.data_ptr() + idx * (k * Lt), received.data_ptr() + idx * (k * Lt)])
+    outs = np.concatenate([enc_out.data_ptr() + idx * (m * Lt), out.data_ptr() + idx * (k * Lt)])
+    indices = np.zeros((2 * n, k), np.uint16)
+    indices[n:] = recv
+    b.set_arrays(op, np.full(2 * n, eng), np.full(2 * n, k), np.full(2 * n, m), np.full(2 * n, Lt), ins, outs,
+                 indices=indices)
+    b.run(graph=True)
+    torch.cuda.synchronize()
+    ok &= bool(torch.equal(out, data)) and bool(torch.equal(enc_out, reps))
+    t = time_ms(torch, lambda: b.run(graph=True), 10)
+    goodput = 2 * n * k * Lt
+    algo = n * (k + m) * Lt + n * 2 * k * Lt
+    return {"workload": f"{n} tower encodes + {n} tower decodes (k={k} m={m} L={Lt}, 8 data symbols erased) in one "
+                        "stripe batch: plan launch + persistent drain (mxk_kernel<1>), CUDA graph",
+            "GBps": round(goodput / t / 1e6, 1), "ms": round(t, 3), "launches": b.last_launches,
+            "roofline": roofline_of(algo, t, "tower plan + persistent tower drain"), "bit_exact": ok}
 
 
 def cpu_encode_tower(cpu, p, h_data):
@@ -951,7 +1005,67 @@ def extra_afft(torch, api, cpu=None):
     return res
 
 
-EXTRAS = {"batched_vs_plain_cfg4": extra_mixed, "latency_cfg1": extra_latency, "tower_cfg2": extra_tower,
+def extra_sweep(torch, api, cpu=None, ks=(10, 32, 64), ms=(4, 8, 16), Ls=4096, in_bytes=512 << 20):
+    """The GF(256) envelope: for each (k, m), a batch of Good Cauchy stripes
+    (L = 4 KiB, enough stripes for about 512 MB of input, far above L2) run
+    as encodes and, separately, as batch decodes from seeded random k-of-n
+    receipt sets, each as one persistent launch.  Per cell: the drain's
+    CUDA-event time (plan launch excluded), its algorithmic bytes ((k+m)*L per
+    encode, 2*k*L per decode) and HBM fraction, and which drain ran (the
+    matrix-specialised encode kernel where eligible)."""
+    from scrs_b200.api import Engine
+    from scrs_b200.batch import OP_DECODE, OP_ENCODE, StripeBatch
+
+    peak = peaks()[0]
+    eng = int(Engine.GOOD_CAUCHY)
+    cells, ok = [], True
+    for k in ks:
+        for m in ms:
+            n = max(1, in_bytes // (k * Ls))
+            gen = torch.Generator(device="cuda")
+            gen.manual_seed(SEED + 100 + k * 17 + m)
+            data = torch.randint(0, 256, (n, k * Ls), dtype=torch.uint8, device="cuda", generator=gen)
+            reps = torch.zeros((n, m * Ls), dtype=torch.uint8, device="cuda")
+            idx = np.arange(n, dtype=np.uint64)
+            b = StripeBatch(api.lib, n)
+            b.set_arrays(np.full(n, OP_ENCODE), np.full(n, eng), np.full(n, k), np.full(n, m), np.full(n, Ls),
+                         data.data_ptr() + idx * (k * Ls), reps.data_ptr() + idx * (m * Ls))
+            b.run()
+            torch.cuda.synchronize()
+            enc = [b.run_timed_drains() for _ in range(5)]
+            t_enc = float(np.median([r[1] + r[2] for r in enc]))
+            spec = b.jit_stripes > 0
+            rng = np.random.default_rng(SEED + 200 + k * 17 + m)
+            recv = np.argsort(rng.random((n, k + m)), axis=1)[:, :k].astype(np.int64)
+            word = torch.cat([data.view(n, k, Ls), reps.view(n, m, Ls)], dim=1)
+            received = word[torch.arange(n, device="cuda")[:, None], torch.from_numpy(recv).cuda()].reshape(n, k * Ls)
+            del word
+            out = torch.zeros((n, k * Ls), dtype=torch.uint8, device="cuda")
+            b.set_arrays(np.full(n, OP_DECODE), np.full(n, eng), np.full(n, k), np.full(n, m), np.full(n, Ls),
+                         received.data_ptr() + idx * (k * Ls), out.data_ptr() + idx * (k * Ls),
+                         indices=recv.astype(np.uint16))
+            b.run()
+            torch.cuda.synchronize()
+            ok &= bool(torch.equal(out, data))
+            dec = [b.run_timed_drains() for _ in range(5)]
+            t_dec = float(np.median([r[2] for r in dec]))
+            plan = float(np.median([r[0] for r in dec]))
+            b.check()
+            enc_bytes, dec_bytes = n * (k + m) * Ls, n * 2 * k * Ls
+            cells.append({"k": k, "m": m, "stripes": n,
+                          "encode_ms": round(t_enc, 4), "encode_frac": round(enc_bytes / t_enc / 1e6 / peak, 3),
+                          "encode_kernel": "scrs_spec_drain" if spec else "mxk_kernel<0>",
+                          "decode_ms": round(t_dec, 4), "decode_frac": round(dec_bytes / t_dec / 1e6 / peak, 3),
+                          "decode_plan_ms": round(plan, 4),
+                          "mean_erased": round(float((recv >= k).sum()) / n, 2)})
+            del data, reps, received, out, b
+            torch.cuda.empty_cache()
+    return {"workload": "Good Cauchy stripes, L=4096, ~512 MB of input per cell; encode and batch decode (seeded "
+                        "random k-of-n receipt sets) as persistent launches; drain time by CUDA events",
+            "peak_GBps": peak, "cells": cells, "bit_exact": ok}
+
+
+EXTRAS = {"batched_vs_plain_cfg4": extra_mixed, "gf256_envelope": extra_sweep, "latency_cfg1": extra_latency, "tower_cfg2": extra_tower,
           "afft_cfg3": extra_afft, "serving_cfg5": extra_serving}
 
 

@@ -347,18 +347,22 @@ SCRS_API int32_t scrs_dec_finalize_into_with_device(scrs_decoder* dec, uint8_t* 
                                            scrs_decode_scratch* scratch,
                                            void* stream, scrs_error* err);
 
-/* ---- Batched GF(256) stripes in one persistent launch ------------------
+/* ---- Batched GF(256) and tower stripes in one persistent launch ---------
  * No single reference counterpart: this runs many independent
  * BatchCodec::encode_into (batch/codec.rs:156) and
  * BatchCodec::decode_into_with (batch/codec.rs:278) calls of uneven
- * geometry as one device work queue.  Per-stripe decode matrices are built
- * on the device.  All pointers in a stripe descriptor are device pointers
- * except `indices`, which is host memory read during submit. */
+ * geometry as one device work queue, and tower stripes likewise: a tower
+ * encode gives the repairs of k in-order feeds (tower/encoder.rs:89-131), a
+ * tower decode the lazy decoder's reconstruction (tower/decoder.rs:218-546).
+ * Per-stripe decode matrices are built on the device; GF(256) and tower
+ * stripes drain through one persistent kernel per field.  All pointers in a
+ * stripe descriptor are device pointers except `indices`, which is host
+ * memory read during submit. */
 enum { SCRS_OP_ENCODE = 0, SCRS_OP_DECODE = 1 };
 
 typedef struct scrs_stripe_desc {
     int32_t op;     /* SCRS_OP_ENCODE or SCRS_OP_DECODE                     */
-    int32_t engine; /* SCRS_ENGINE_STANDARD_CAUCHY or SCRS_ENGINE_GOOD_CAUCHY */
+    int32_t engine; /* SCRS_ENGINE_STANDARD_CAUCHY, _GOOD_CAUCHY or _TOWER     */
     uint32_t k;
     uint32_t m;
     uint64_t symbol_len;
@@ -397,7 +401,8 @@ SCRS_API int32_t scrs_stripe_batch_set(scrs_stripe_batch* batch,
  * stripe with r data symbols erased (BatchCodec writes the present rows into
  * the output the same way, batch/codec.rs:323-324).  In this mode
  * scrs_stripe_batch_run returns once every output is in its host buffer, and
- * use_graph is ignored. */
+ * use_graph is ignored.  Host-buffer batches take GF(256) stripes only (a
+ * tower stripe: SCRS_ERR_BAD_ARGUMENT, a = 2). */
 SCRS_API int32_t scrs_stripe_batch_set_host(scrs_stripe_batch* batch,
                                             const scrs_stripe_desc* descs,
                                             uint64_t count, scrs_error* err);
@@ -508,7 +513,7 @@ SCRS_API void scrs_tune_table_clear(void);
  * of every engine are submitted with device-resident inputs and outputs and
  * admitted first come, first served as one of `slots` streams and the device
  * memory budget free up; admitted work overlaps on the device.  Waiting
- * GF(256) requests are coalesced into one stripe batch per slot; tower and
+ * GF(256) and tower requests are coalesced into one stripe batch per slot;
  * additive-FFT requests take a slot each and use engines kept resident per
  * slot (least recently used profiles are evicted).  The budget counts every
  * admitted request's input and output bytes plus estimated resident engine
@@ -554,12 +559,14 @@ SCRS_API int32_t scrs_server_submit(scrs_server* server, const scrs_request* req
 SCRS_API int32_t scrs_server_progress(scrs_server* server, scrs_completion* done,
                                       uint32_t capacity, uint32_t* n_done,
                                       scrs_error* err);
-/* Build the resident engines of one tower or additive-FFT profile for `op`
+/* Build the resident engines of one additive-FFT profile for `op`
  * on every slot, so that no request of that profile pays the build (device
  * allocations, which stall the whole device) on its way through.  For
  * start-up: SCRS_ERR_BAD_ARGUMENT (a = 3) while any slot is running
  * requests, (a = 1) for a GF(256) engine (its stripe batches need no
- * resident engines).  Resident engines count against the memory budget and
+ * resident engines); SCRS_OK with nothing built for a tower profile (tower
+ * requests run in the stripe batches too).  Resident engines count against
+ * the memory budget and
  * each slot keeps at most 8 profiles, least recently used evicted first. */
 SCRS_API int32_t scrs_server_reserve(scrs_server* server, int32_t op, int32_t engine,
                                      uint64_t k, uint64_t m, uint64_t symbol_len,

@@ -107,13 +107,21 @@ struct scrs_stripe_batch {
     DevBuf d_tasks, d_plans, d_counter, d_arena, d_item_task;
     std::vector<uint32_t> item_task;
     std::vector<MxkTask> tasks;
-    std::vector<CauchyPlanTask> plans;
+    std::vector<CauchyPlanTask> plans;    // GF(256) decode plans, then (from plans16_lo) the tower ones
+    std::vector<uint8_t> task_gf16;       // per task: a tower stripe
     std::vector<uint8_t> arena;
     uint32_t total_items = 0, max_in = 1, max_plan_r = 0;
-    scrs_tune_key key{};  // geometry key of the current descriptors (autotuner table)
+    // Tower stripes (GF((2^8)^2)) take the items [gen_hi, total_items) and
+    // their own persistent drain; their plans are plans[plans16_lo, end).
+    uint32_t gen_hi = 0, max_in16 = 1, max_plan_r16 = 0, plans16_lo = 0;
+    int shape16 = kShapeAny;
+    std::map<std::pair<uint32_t, uint32_t>, std::vector<uint16_t>> tower_coef;  // host tables by (k, m)
+    std::vector<uint16_t> l_row_of, l_missing, l_present, l_repairs;  // per-stripe list scratch
+    std::vector<uint8_t> l_seen;
+    scrs_tune_key key{};  // geometry key of the current GF(256) descriptors (autotuner table)
     // Encode groups of one (engine, k, m) run through a kernel specialised to
     // their matrix (jit.cu): items [item_lo, item_hi) each; the generic drain
-    // takes items [gen_lo, total_items).
+    // takes items [gen_lo, gen_hi).
     struct SpecRun {
         JitKernel jk;
         uint32_t item_lo, item_hi;
@@ -183,6 +191,30 @@ struct scrs_stripe_batch {
 namespace {
 constexpr size_t kMaxPieces = 16;  // one work counter each in d_counter
 constexpr size_t kMaxSpecRuns = 4;  // specialised groups per batch (counters 1..4)
+constexpr size_t kTowerCounter = 1 + kMaxSpecRuns;  // work counter of the tower drain
+
+// g^i for i < 65535 (tower/cauchy.rs:44-49) on the current device: the x and
+// y coordinates every tower decode plan reads.  Uploaded once per device.
+cudaError_t tower_powers_table(const uint16_t** out) {
+    static std::mutex mu;
+    static std::map<int, std::unique_ptr<DevBuf>> tables;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = tables.find(dev);
+    if (it == tables.end()) {
+        std::vector<uint16_t> pw(65535);
+        hf::tower_powers(65535, pw.data());
+        std::unique_ptr<DevBuf> t(new (std::nothrow) DevBuf());
+        if (!t) return cudaErrorMemoryAllocation;
+        if ((e = t->ensure(65535 * 2)) != cudaSuccess || (e = upload_now(t->p, pw.data(), 65535 * 2)) != cudaSuccess)
+            return e;
+        it = tables.emplace(dev, std::move(t)).first;
+    }
+    *out = it->second->as<uint16_t>();
+    return cudaSuccess;
+}
 // A group is specialised when it has at least one persistent grid of items
 // (this many CTAs per SM on every SM).
 constexpr uint64_t kJitMinCtasPerSm = 8;
@@ -273,29 +305,34 @@ int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc
     // ---- validate and size the arena: [encode coefficient tables][decode slots]
     size_t coef_bytes = 0, slot_bytes = 0;
     std::map<std::tuple<int, uint32_t, uint32_t>, size_t> coef_off;
-    uint64_t items = 0;
+    uint64_t items = 0, n_tower = 0;
     auto align16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
     for (uint64_t s = 0; s < count; s++) {
         const scrs_stripe_desc& d = descs[s];
         if (d.op != SCRS_OP_ENCODE && d.op != SCRS_OP_DECODE) return set_err(err, SCRS_ERR_BAD_ARGUMENT, 1, s);
-        if (d.engine != SCRS_ENGINE_STANDARD_CAUCHY && d.engine != SCRS_ENGINE_GOOD_CAUCHY)
+        const bool gf16 = d.engine == SCRS_ENGINE_TOWER;
+        if (d.engine != SCRS_ENGINE_STANDARD_CAUCHY && d.engine != SCRS_ENGINE_GOOD_CAUCHY && !gf16)
             return set_err(err, SCRS_ERR_BAD_ARGUMENT, 2, s);
         if (d.k == 0 || d.m == 0) return set_err(err, SCRS_CONFIG_ZERO_DIMENSION, 0, s);
         if (d.symbol_len == 0) return set_err(err, SCRS_CONFIG_ZERO_SYMBOL_LEN, 0, s);
-        const uint64_t cap = d.engine == SCRS_ENGINE_STANDARD_CAUCHY ? 256 : 255;
+        if (gf16 && d.symbol_len % 2) return set_err(err, SCRS_CONFIG_ODD_SYMBOL_LEN, 0, s);
+        const uint64_t cap = d.engine == SCRS_ENGINE_STANDARD_CAUCHY ? 256 : gf16 ? 65535 : 255;
         if ((uint64_t)d.k + d.m > cap) return set_err(err, SCRS_CONFIG_TOO_MANY_SYMBOLS, cap, s);
         if (!d.in || !d.out) return set_err(err, SCRS_ERR_NULL_ARGUMENT, 0, s);
-        items += n_chunks(d.symbol_len, false);
+        const size_t elem = gf16 ? 2 : 1;
+        n_tower += gf16;
+        items += n_chunks(d.symbol_len, gf16);
         if (d.op == SCRS_OP_ENCODE) {
             auto key = std::make_tuple(d.engine, d.k, d.m);
             if (!coef_off.count(key)) {
                 coef_off[key] = coef_bytes;
-                coef_bytes = align16(coef_bytes + (size_t)d.k * d.m);
+                coef_bytes = align16(coef_bytes + (size_t)d.k * d.m * elem);
             }
         } else {
             if (!d.indices) return set_err(err, SCRS_ERR_NULL_ARGUMENT, 0, s);
             const uint32_t n = d.k + d.m;
-            uint8_t seen[256] = {0};
+            std::vector<uint8_t>& seen = b->l_seen;
+            seen.assign(n, 0);
             uint32_t r = 0;
             for (uint32_t q = 0; q < d.k; q++) {
                 uint32_t i = d.indices[q];
@@ -306,25 +343,45 @@ int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc
             }
             // lists: in_rows[k] pass_rows[k] out_rows[r] missing[r] repairs[r] present[k-r]; coef[k*r]
             slot_bytes = align16(slot_bytes + 2 * ((size_t)3 * d.k + 3 * r));
-            slot_bytes = align16(slot_bytes + (size_t)d.k * std::max<uint32_t>(r, 1));
+            slot_bytes = align16(slot_bytes + (size_t)d.k * std::max<uint32_t>(r, 1) * elem);
         }
     }
     if (items > b->max_items || items > 0xFFFFFFFFull) return set_err(err, SCRS_ERR_CAPACITY, items, b->max_items);
+    if (n_tower && b->compact_decode) return set_err(err, SCRS_ERR_BAD_ARGUMENT, 2);  // host-buffer batches: GF(256)
+    const uint16_t* d_powers = nullptr;
+    if (n_tower) SCRS_CUDA(tower_powers_table(&d_powers));
     const size_t arena_bytes = coef_bytes + slot_bytes;
     b->arena.assign(arena_bytes + 16, 0);
     SCRS_CUDA(b->d_arena.ensure_grow(b->arena.size()));
     uint8_t* dbase = b->d_arena.as<uint8_t>();
-    for (auto& kv : coef_off)
-        hf::gf8_coefficients(std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first),
-                             b->arena.data() + kv.second);
-    // ---- tasks
+    for (auto& kv : coef_off) {
+        const int engine = std::get<0>(kv.first);
+        const uint32_t k = std::get<1>(kv.first), m = std::get<2>(kv.first);
+        if (engine == SCRS_ENGINE_TOWER) {  // tower/cauchy.rs:69-106, cached per geometry
+            std::vector<uint16_t>& t = b->tower_coef[std::make_pair(k, m)];
+            if (t.empty()) {
+                std::vector<uint16_t> pw(k + m);
+                hf::tower_powers(k + m, pw.data());
+                t.resize((size_t)k * m);
+                hf::tower_coefficients(k, m, pw.data(), t.data());
+            }
+            memcpy(b->arena.data() + kv.second, t.data(), t.size() * 2);
+        } else {
+            hf::gf8_coefficients(engine, k, m, b->arena.data() + kv.second);
+        }
+    }
+    // ---- tasks (tower plans are kept apart, then appended after the GF(256) ones)
     b->tasks.clear();
+    b->task_gf16.clear();
     b->plans.clear();
+    std::vector<CauchyPlanTask> plans16;
     b->plan_begin.assign(count + 1, 0);
     size_t off = coef_bytes;  // decode slots follow the coefficient tables
-    uint32_t item = 0, max_in = 1, max_r = 0;
+    uint32_t max_r = 0, max_r16 = 0;
     for (uint64_t s = 0; s < count; s++) {
         const scrs_stripe_desc& d = descs[s];
+        const bool gf16 = d.engine == SCRS_ENGINE_TOWER;
+        const size_t elem = gf16 ? 2 : 1;
         b->plan_begin[s] = (uint32_t)b->plans.size();
         MxkTask T{};
         T.in = d.in;
@@ -333,28 +390,25 @@ int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc
         T.in_stride = d.symbol_len;
         T.out_stride = d.symbol_len;
         T.n_in = d.k;
-        T.n_items = n_chunks(d.symbol_len, false);
-        T.item_begin = item;
+        T.n_items = n_chunks(d.symbol_len, gf16);
         T.aligned = (d.symbol_len % 16 == 0 && aligned16(d.in) && aligned16(d.out)) ? 1u : 0u;
         if (d.op == SCRS_OP_ENCODE) {
             T.coef = dbase + coef_off[std::make_tuple(d.engine, d.k, d.m)];
             T.n_out = d.m;
             T.ld = d.m;
         } else {
-            // k + m <= 256 (validated above): fixed-size lists, no allocation per stripe
             const uint32_t k = d.k, n = d.k + d.m;
-            uint16_t row_of[256], missing[256], present[256], repairs[256];
-            std::fill(row_of, row_of + n, kNoRow);
+            std::vector<uint16_t>&row_of = b->l_row_of, &missing = b->l_missing, &present = b->l_present,
+                                 &repairs = b->l_repairs;
+            row_of.assign(n, kNoRow);
+            missing.clear();
+            present.clear();
+            repairs.clear();
             for (uint32_t q = 0; q < k; q++) row_of[d.indices[q]] = (uint16_t)q;
-            uint32_t r = 0, p = 0, nrep = 0;
-            for (uint32_t i = 0; i < k; i++) {
-                if (row_of[i] != kNoRow)
-                    present[p++] = (uint16_t)i;
-                else
-                    missing[r++] = (uint16_t)i;
-            }
+            for (uint32_t i = 0; i < k; i++) (row_of[i] != kNoRow ? present : missing).push_back((uint16_t)i);
             for (uint32_t j = 0; j < d.m; j++)
-                if (row_of[k + j] != kNoRow) repairs[nrep++] = (uint16_t)j;
+                if (row_of[k + j] != kNoRow) repairs.push_back((uint16_t)j);
+            const uint32_t r = (uint32_t)missing.size(), p = (uint32_t)present.size();
             uint16_t* L16 = reinterpret_cast<uint16_t*>(b->arena.data() + off);
             uint16_t* in_rows = L16;
             uint16_t* pass_rows = L16 + k;
@@ -364,15 +418,15 @@ int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc
             uint16_t* l_present = l_repairs + r;
             for (uint32_t t = 0; t < r; t++) in_rows[t] = row_of[k + repairs[t]], pass_rows[t] = kNoRow;
             for (uint32_t z = 0; z < p; z++) in_rows[r + z] = row_of[present[z]], pass_rows[r + z] = present[z];
-            std::copy(missing, missing + r, out_rows);
-            std::copy(missing, missing + r, l_missing);
-            std::copy(repairs, repairs + nrep, l_repairs);
-            std::copy(present, present + p, l_present);
+            std::copy(missing.begin(), missing.end(), out_rows);
+            std::copy(missing.begin(), missing.end(), l_missing);
+            std::copy(repairs.begin(), repairs.end(), l_repairs);
+            std::copy(present.begin(), present.end(), l_present);
             const size_t dl = (size_t)(reinterpret_cast<uint8_t*>(L16) - b->arena.data());
             uint16_t* dL16 = reinterpret_cast<uint16_t*>(dbase + dl);
             off = align16(off + 2 * ((size_t)3 * k + 3 * r));
             uint8_t* dcoef = dbase + off;
-            off = align16(off + (size_t)k * std::max<uint32_t>(r, 1));
+            off = align16(off + (size_t)k * std::max<uint32_t>(r, 1) * elem);
             T.in_rows = dL16;
             // compact (host-buffer batches): the r missing rows only, as rows
             // 0..r-1 of `out`; the present rows never leave the host
@@ -391,35 +445,49 @@ int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc
                 P.missing = dL16 + 2 * k + r;
                 P.repairs = dL16 + 2 * k + 2 * r;
                 P.present = dL16 + 2 * k + 3 * r;
+                P.powers = gf16 ? d_powers : nullptr;
                 P.coef = dcoef;
-                b->plans.push_back(P);
-                max_r = std::max(max_r, r);
+                if (gf16) {
+                    plans16.push_back(P);
+                    max_r16 = std::max(max_r16, r);
+                } else {
+                    b->plans.push_back(P);
+                    max_r = std::max(max_r, r);
+                }
             }
         }
-        max_in = std::max(max_in, T.n_in);
-        item += T.n_items;
         b->tasks.push_back(T);
+        b->task_gf16.push_back(gf16 ? 1 : 0);
     }
     b->plan_begin[count] = (uint32_t)b->plans.size();
-    b->total_items = item;
-    b->max_in = max_in;
-    b->key = tune_key_of(descs, count);
-    // ---- encode groups with a specialised kernel take the first item ranges
+    b->plans16_lo = (uint32_t)b->plans.size();
+    b->plans.insert(b->plans.end(), plans16.begin(), plans16.end());
+    b->max_plan_r = max_r;
+    b->max_plan_r16 = max_r16;
+    if (n_tower) {  // the autotuner's key describes the GF(256) stripes (the drain it tunes)
+        std::vector<scrs_stripe_desc> gf8;
+        for (uint64_t s = 0; s < count; s++)
+            if (descs[s].engine != SCRS_ENGINE_TOWER) gf8.push_back(descs[s]);
+        b->key = tune_key_of(gf8.data(), gf8.size());
+    } else {
+        b->key = tune_key_of(descs, count);
+    }
+    // ---- items: specialised GF(256) encode groups, the generic GF(256)
+    // drain's tasks, then the tower tasks (each task in stripe order)
     b->spec.clear();
-    b->gen_lo = 0;
+    std::vector<char> in_spec(count, 0);
+    uint32_t next = 0;
     if (b->jit) {
         std::map<std::tuple<int, uint32_t, uint32_t>, std::vector<uint32_t>> groups;
         std::vector<std::tuple<int, uint32_t, uint32_t>> order;  // first appearance
         for (uint64_t s = 0; s < count; s++) {
             const scrs_stripe_desc& d = descs[s];
-            if (d.op != SCRS_OP_ENCODE || !jit_eligible(d.k, d.m)) continue;
+            if (d.op != SCRS_OP_ENCODE || d.engine == SCRS_ENGINE_TOWER || !jit_eligible(d.k, d.m)) continue;
             auto key = std::make_tuple(d.engine, d.k, d.m);
             auto& g = groups[key];
             if (g.empty()) order.push_back(key);
             g.push_back((uint32_t)s);
         }
-        std::vector<char> in_spec(count, 0);
-        uint32_t next = 0;
         for (auto& key : order) {
             if (b->spec.size() == kMaxSpecRuns) break;
             auto& g = groups[key];
@@ -438,35 +506,44 @@ int32_t scrs::stripe_batch_set_impl(scrs_stripe_batch* b, const scrs_stripe_desc
             }
             b->spec.push_back({jk, lo, next, (uint64_t)g.size()});
         }
-        if (!b->spec.empty()) {
-            b->gen_lo = next;
-            uint32_t gen_max_in = 1;
-            for (uint64_t t = 0; t < count; t++) {
-                if (in_spec[t]) continue;
-                b->tasks[t].item_begin = next;
-                next += b->tasks[t].n_items;
-                gen_max_in = std::max(gen_max_in, b->tasks[t].n_in);
-            }
-            b->max_in = gen_max_in;
-        }
     }
-    const bool all_aligned =
-        std::all_of(b->tasks.begin(), b->tasks.end(), [](const MxkTask& T) { return T.aligned != 0; });
-    const bool all_whole = std::all_of(b->tasks.begin(), b->tasks.end(),
-                                       [](const MxkTask& T) { return T.L % FieldGeom<0>::kChunk == 0; });
-    b->shape = !all_aligned ? kShapeAny : all_whole ? (kShapeAligned | kShapeWhole) : kShapeAligned;
-    b->item_task.resize(item);
+    b->gen_lo = next;
+    uint32_t max_in = 1, max_in16 = 1;
+    for (int pass = 0; pass < 2; pass++) {
+        for (uint64_t t = 0; t < count; t++) {
+            if (in_spec[t] || b->task_gf16[t] != pass) continue;
+            b->tasks[t].item_begin = next;
+            next += b->tasks[t].n_items;
+            uint32_t& mx = pass ? max_in16 : max_in;
+            mx = std::max(mx, b->tasks[t].n_in);
+        }
+        if (pass == 0) b->gen_hi = next;
+    }
+    b->total_items = next;
+    b->max_in = max_in;
+    b->max_in16 = max_in16;
+    auto shape_of = [&](uint8_t gf16) {
+        bool all_aligned = true, all_whole = true;
+        for (size_t t = 0; t < b->tasks.size(); t++) {
+            if (b->task_gf16[t] != gf16) continue;
+            all_aligned &= b->tasks[t].aligned != 0;
+            all_whole &= b->tasks[t].L % FieldGeom<0>::kChunk == 0;
+        }
+        return !all_aligned ? kShapeAny : all_whole ? (kShapeAligned | kShapeWhole) : kShapeAligned;
+    };
+    b->shape = shape_of(0);
+    b->shape16 = shape_of(1);
+    b->item_task.resize(next);
     for (size_t t = 0; t < b->tasks.size(); t++)
         std::fill(b->item_task.begin() + b->tasks[t].item_begin,
                   b->item_task.begin() + b->tasks[t].item_begin + b->tasks[t].n_items, (uint32_t)t);
-    SCRS_CUDA(b->d_item_task.ensure_grow((size_t)item * 4));
-    b->max_plan_r = max_r;
+    SCRS_CUDA(b->d_item_task.ensure_grow((size_t)next * 4));
     if (off > arena_bytes) return set_err(err, SCRS_ERR_CAPACITY, off, arena_bytes);  // layout invariant
     struct Up {
         void* dst;
         const void* src;
         size_t bytes;
-    } ups[4] = {{b->d_item_task.p, b->item_task.data(), (size_t)item * 4},
+    } ups[4] = {{b->d_item_task.p, b->item_task.data(), (size_t)next * 4},
                 {b->d_arena.p, b->arena.data(), b->arena.size()},
                 {b->d_tasks.p, b->tasks.data(), b->tasks.size() * sizeof(MxkTask)},
                 {b->d_plans.p, b->plans.data(), b->plans.size() * sizeof(CauchyPlanTask)}};
@@ -693,7 +770,18 @@ DrainCfg drain_cfg(const scrs_stripe_batch* b) {
     }
     const int fit = mxk_ctas_per_sm(c.seg_rows, drain_shape(b, c.seg_rows));
     if (c.ctas_per_sm <= 0 || c.ctas_per_sm > fit) c.ctas_per_sm = fit;
-    const uint32_t items = b->total_items - b->gen_lo;
+    const uint32_t items = b->gen_hi - b->gen_lo;
+    c.grid = std::max(1, std::min<int>(b->sm_count * c.ctas_per_sm, (int)std::max<uint32_t>(items, 1)));
+    return c;
+}
+
+// The tower stripes' drain: all their inputs per segment up to 16 rows, the
+// most CTAs per SM that fit.
+DrainCfg drain_cfg16(const scrs_stripe_batch* b) {
+    DrainCfg c{std::max(1, std::min((int)b->max_in16, FieldGeom<1>::kSegMax)), 0, 0};
+    const int shape = b->shape16 | ((int)b->max_in16 <= c.seg_rows ? kShapeOneSeg : 0);
+    c.ctas_per_sm = mxk_ctas_per_sm(c.seg_rows, shape, 1);
+    const uint32_t items = b->total_items - b->gen_hi;
     c.grid = std::max(1, std::min<int>(b->sm_count * c.ctas_per_sm, (int)std::max<uint32_t>(items, 1)));
     return c;
 }
@@ -708,11 +796,33 @@ int32_t enqueue_drains(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err, b
                              b->d_counter.as<uint32_t>() + 1 + q, b->status.dev, b->sm_count * R.jk.ctas_per_sm, st));
         b->last_launches++;
     }
-    if (run_generic && b->total_items > b->gen_lo) {
+    if (run_generic && b->gen_hi > b->gen_lo) {
         const DrainCfg c = drain_cfg(b);
-        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), b->gen_lo,
-                                   b->total_items, b->d_counter.as<uint32_t>(), b->status.dev, c.seg_rows, c.grid,
-                                   st, drain_shape(b, c.seg_rows)));
+        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), b->gen_lo, b->gen_hi,
+                                   b->d_counter.as<uint32_t>(), b->status.dev, c.seg_rows, c.grid, st,
+                                   drain_shape(b, c.seg_rows)));
+        b->last_launches++;
+    }
+    if (run_generic && b->total_items > b->gen_hi) {
+        const DrainCfg c = drain_cfg16(b);
+        const int shape = b->shape16 | ((int)b->max_in16 <= c.seg_rows ? kShapeOneSeg : 0);
+        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), b->gen_hi,
+                                   b->total_items, b->d_counter.as<uint32_t>() + kTowerCounter, b->status.dev,
+                                   c.seg_rows, c.grid, st, shape, 1));
+        b->last_launches++;
+    }
+    return SCRS_OK;
+}
+
+// The decode plans: GF(256) ones, then tower ones.
+int32_t enqueue_plans(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
+    if (b->plans16_lo) {
+        SCRS_CUDA(launch_cauchy_plan(b->d_plans.as<CauchyPlanTask>(), b->plans16_lo, 0, b->max_plan_r, st));
+        b->last_launches++;
+    }
+    if (b->plans.size() > b->plans16_lo) {
+        SCRS_CUDA(launch_cauchy_plan(b->d_plans.as<CauchyPlanTask>() + b->plans16_lo,
+                                     (uint32_t)b->plans.size() - b->plans16_lo, 1, b->max_plan_r16, st));
         b->last_launches++;
     }
     return SCRS_OK;
@@ -724,7 +834,7 @@ int32_t enqueue_drains(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err, b
 // specialised drains' tails leave idle; the drains touch disjoint items and
 // outputs.  Under graph capture the fork and join become graph edges.
 int32_t enqueue_batch(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
-    SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, (1 + b->spec.size()) * sizeof(uint32_t), st));
+    SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, (kTowerCounter + 1) * sizeof(uint32_t), st));
     b->last_launches = 0;
     const bool fork = !b->spec.empty() && b->total_items > b->gen_lo;
     if (fork) {
@@ -733,10 +843,8 @@ int32_t enqueue_batch(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
         int32_t r = enqueue_drains(b, b->s_fork, err, true, false);
         if (r) return r;
     }
-    if (!b->plans.empty()) {
-        SCRS_CUDA(launch_cauchy_plan(b->d_plans.as<CauchyPlanTask>(), (uint32_t)b->plans.size(), 0, b->max_plan_r, st));
-        b->last_launches++;
-    }
+    int32_t rp = enqueue_plans(b, st, err);
+    if (rp) return rp;
     if (!fork) return enqueue_drains(b, st, err);
     int32_t r = enqueue_drains(b, st, err, false, true);
     if (r) return r;
@@ -883,14 +991,17 @@ extern "C" int32_t scrs_stripe_batch_run_plain(scrs_stripe_batch* b, void* strea
     int32_t r0 = copy_in(b, st, err);
     if (r0) return r0;
     b->last_launches = 0;
-    size_t pi = 0;
-    for (const MxkTask& T : b->tasks) {
+    size_t pi[2] = {0, b->plans16_lo};  // next plan of each field
+    const size_t pend[2] = {b->plans16_lo, b->plans.size()};
+    for (size_t t = 0; t < b->tasks.size(); t++) {
+        const MxkTask& T = b->tasks[t];
+        const int f = b->task_gf16[t];
         // decode stripes carry row lists (encodes none); with erasures they have a plan
-        if (T.in_rows && T.n_out && pi < b->plans.size()) {
-            SCRS_CUDA(launch_cauchy_plan_single(b->plans[pi++], 0, st));
+        if (T.in_rows && T.n_out && pi[f] < pend[f]) {
+            SCRS_CUDA(launch_cauchy_plan_single(b->plans[pi[f]++], f, st));
             b->last_launches++;
         }
-        SCRS_CUDA(launch_mxk_single(T, 0, b->status.dev, 0, st));
+        SCRS_CUDA(launch_mxk_single(T, f, b->status.dev, 0, st));
         b->last_launches++;
     }
     r0 = copy_out(b, st, err);
@@ -917,13 +1028,11 @@ extern "C" int32_t scrs_stripe_batch_run_timed_drains(scrs_stripe_batch* b, void
     cudaStream_t st = (cudaStream_t)stream;
     cudaEvent_t ev[4];
     for (auto& e : ev) SCRS_CUDA(cudaEventCreate(&e));
-    SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, (1 + b->spec.size()) * sizeof(uint32_t), st));
+    SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, (kTowerCounter + 1) * sizeof(uint32_t), st));
     b->last_launches = 0;
     cudaEventRecord(ev[0], st);
-    if (!b->plans.empty()) {
-        SCRS_CUDA(launch_cauchy_plan(b->d_plans.as<CauchyPlanTask>(), (uint32_t)b->plans.size(), 0, b->max_plan_r, st));
-        b->last_launches++;
-    }
+    int32_t rp = enqueue_plans(b, st, err);
+    if (rp) return rp;
     cudaEventRecord(ev[1], st);
     int32_t rc = enqueue_drains(b, st, err, false, true);
     if (rc) return rc;
@@ -971,8 +1080,8 @@ int32_t time_drain(scrs_stripe_batch* b, cudaStream_t st, int seg_rows, int grid
     for (uint32_t rep = 0; rep <= reps; rep++) {
         SCRS_CUDA(cudaMemsetAsync(b->d_counter.p, 0, 4, st));
         SCRS_CUDA(cudaEventRecord(e0, st));
-        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), b->gen_lo,
-                                   b->total_items, b->d_counter.as<uint32_t>(), b->status.dev, seg_rows, grid, st,
+        SCRS_CUDA(launch_gf256_mxk(b->d_tasks.as<MxkTask>(), b->d_item_task.as<uint32_t>(), b->gen_lo, b->gen_hi,
+                                   b->d_counter.as<uint32_t>(), b->status.dev, seg_rows, grid, st,
                                    drain_shape(b, seg_rows)));
         SCRS_CUDA(cudaEventRecord(e1, st));
         SCRS_CUDA(cudaEventSynchronize(e1));
@@ -993,13 +1102,14 @@ extern "C" int32_t scrs_stripe_batch_autotune(scrs_stripe_batch* b, void* stream
     if (reps > 100) return set_err(err, SCRS_ERR_BAD_ARGUMENT, 3, reps);
     if (reps == 0) reps = 5;
     cudaStream_t st = (cudaStream_t)stream;
-    if (b->total_items <= b->gen_lo) return scrs_stripe_batch_launch_params(b, chosen, err);
+    if (b->gen_hi <= b->gen_lo) return scrs_stripe_batch_launch_params(b, chosen, err);
     // inputs on the device and decode matrices built before any drain
     if (b->host_mode) {
         int32_t r = run_host(b, st, err);
         if (r) return r;
-    } else if (!b->plans.empty()) {
-        SCRS_CUDA(launch_cauchy_plan(b->d_plans.as<CauchyPlanTask>(), (uint32_t)b->plans.size(), 0, b->max_plan_r, st));
+    } else {
+        int32_t r = enqueue_plans(b, st, err);
+        if (r) return r;
     }
     const int max_seg = std::min<int>((int)b->max_in, FieldGeom<0>::kSegMax);
     const int def_seg = mxk_default_seg((int)b->max_in);
@@ -1021,7 +1131,7 @@ extern "C" int32_t scrs_stripe_batch_autotune(scrs_stripe_batch* b, void* stream
             if (std::find(ctas.begin(), ctas.end(), c) == ctas.end()) ctas.push_back(c);
         }
         for (int c : ctas) {
-            const int grid = std::max(1, std::min<int>(b->sm_count * c, (int)(b->total_items - b->gen_lo)));
+            const int grid = std::max(1, std::min<int>(b->sm_count * c, (int)(b->gen_hi - b->gen_lo)));
             float ms = 0;
             rc = time_drain(b, st, seg, grid, reps, e0, e1, &ms, err);
             if (rc) break;

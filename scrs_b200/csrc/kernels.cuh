@@ -107,9 +107,10 @@ struct CauchyPlanTask {
 // (n_in <= seg_rows and accumulate == 0: no partial sums carried from one
 // segment to the next).
 constexpr int kShapeAny = 0, kShapeAligned = 1, kShapeWhole = 2, kShapeOneSeg = 4;
+// gf16 != 0: tower stripes (GF((2^8)^2), seg_rows at most FieldGeom<1>::kSegMax).
 cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
                              uint32_t* work_counter, int32_t* status, int seg_rows, int grid, cudaStream_t stream,
-                             int shape = kShapeAny);
+                             int shape = kShapeAny, int gf16 = 0);
 // One task by value; grid <= 0 means one CTA per row chunk (or the
 // input-split form for more than one segment of inputs, see below).
 cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream);
@@ -128,9 +129,10 @@ cudaError_t launch_cauchy_plan(const CauchyPlanTask* tasks, uint32_t n_tasks, in
 constexpr uint32_t kPlanSmemMaxR = 12288;
 // Input rows per segment when nothing else is chosen: all of them up to kSeg.
 int mxk_default_seg(int max_in);
-// Most CTAs of the GF(256) persistent drain one SM holds with seg_rows rows
-// staged per segment (shared memory and registers permitting).
-int mxk_ctas_per_sm(int seg_rows, int shape = kShapeAny);
+// Most CTAs of the persistent drain (GF(256), or tower with gf16) one SM
+// holds with seg_rows rows staged per segment (shared memory and registers
+// permitting).
+int mxk_ctas_per_sm(int seg_rows, int shape = kShapeAny, int gf16 = 0);
 // The one-time per-device set-up of the batch kernels (decode-plan tables,
 // shared-memory limits).  Must precede a stream capture of them: the set-up
 // synchronises, which a capturing thread may not do.

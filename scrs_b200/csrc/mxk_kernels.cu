@@ -609,14 +609,21 @@ size_t smem_bytes(int gf16, int seg_rows) {
     return (size_t)kSmemHeader + (size_t)seg * chunk;
 }
 
-// The persistent drain's instantiations, indexed by drain_index(shape).
+// The persistent drain's instantiations, indexed by [field][drain_index(shape)]
+// (GF(256) stripes, tower stripes).
 using DrainFn = void (*)(const MxkTask*, const uint32_t*, uint32_t, uint32_t, uint32_t*, int32_t*, int);
-constexpr DrainFn kDrains[6] = {mxk_kernel<0, kShapeAny>,
-                                mxk_kernel<0, kShapeAligned>,
-                                mxk_kernel<0, kShapeAligned | kShapeWhole>,
-                                mxk_kernel<0, kShapeOneSeg>,
-                                mxk_kernel<0, kShapeOneSeg | kShapeAligned>,
-                                mxk_kernel<0, kShapeOneSeg | kShapeAligned | kShapeWhole>};
+constexpr DrainFn kDrains[2][6] = {{mxk_kernel<0, kShapeAny>,
+                                    mxk_kernel<0, kShapeAligned>,
+                                    mxk_kernel<0, kShapeAligned | kShapeWhole>,
+                                    mxk_kernel<0, kShapeOneSeg>,
+                                    mxk_kernel<0, kShapeOneSeg | kShapeAligned>,
+                                    mxk_kernel<0, kShapeOneSeg | kShapeAligned | kShapeWhole>},
+                                   {mxk_kernel<1, kShapeAny>,
+                                    mxk_kernel<1, kShapeAligned>,
+                                    mxk_kernel<1, kShapeAligned | kShapeWhole>,
+                                    mxk_kernel<1, kShapeOneSeg>,
+                                    mxk_kernel<1, kShapeOneSeg | kShapeAligned>,
+                                    mxk_kernel<1, kShapeOneSeg | kShapeAligned | kShapeWhole>}};
 
 int drain_index(int shape) {
     const bool aligned = shape & kShapeAligned, whole = aligned && (shape & kShapeWhole);
@@ -633,10 +640,8 @@ cudaError_t set_mxk_attrs() {
             cudaFuncSetAttribute(mxk_single_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(mxk_ksplit_kernel<kGf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if constexpr (!kGf16) {  // the persistent drain serves GF(256) stripe batches
-            for (auto fn : kDrains)
-                if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        }
+        for (auto fn : kDrains[kGf16])  // the persistent drains of stripe batches
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         return e;
     });
 }
@@ -699,29 +704,30 @@ int mxk_default_seg(int max_in) { return std::max(1, std::min(max_in, FieldGeom<
 cudaError_t prepare_batch_kernels() {
     cudaError_t e = ensure_tables();
     if (e == cudaSuccess) e = set_mxk_attrs<0>();
+    if (e == cudaSuccess) e = set_mxk_attrs<1>();
     return e;
 }
 
-int mxk_ctas_per_sm(int seg_rows, int shape) {
+int mxk_ctas_per_sm(int seg_rows, int shape, int gf16) {
     int n = 0;
-    if (set_mxk_attrs<0>() != cudaSuccess) return 1;
-    cudaError_t e =
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kDrains[drain_index(shape)], kThreads, smem_bytes(0, seg_rows));
+    if ((gf16 ? set_mxk_attrs<1>() : set_mxk_attrs<0>()) != cudaSuccess) return 1;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kDrains[gf16 ? 1 : 0][drain_index(shape)],
+                                                                  kThreads, smem_bytes(gf16, seg_rows));
     if (e != cudaSuccess || n < 1) n = 1;
     return n;
 }
 
 cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, uint32_t item_lo, uint32_t item_end,
                              uint32_t* counter, int32_t* status, int seg_rows, int grid, cudaStream_t stream,
-                             int shape) {
+                             int shape, int gf16) {
     if (item_end <= item_lo) return cudaSuccess;
-    if (seg_rows < 1 || seg_rows > FieldGeom<0>::kSegMax) return cudaErrorInvalidValue;
-    cudaError_t e = set_mxk_attrs<0>();
+    if (seg_rows < 1 || seg_rows > (gf16 ? FieldGeom<1>::kSegMax : FieldGeom<0>::kSegMax)) return cudaErrorInvalidValue;
+    cudaError_t e = gf16 ? set_mxk_attrs<1>() : set_mxk_attrs<0>();
     if (e != cudaSuccess) return e;
     if (grid <= 0 || grid > (int)(item_end - item_lo)) grid = (int)(item_end - item_lo);
-    const auto fn = kDrains[drain_index(shape)];
-    fn<<<grid, kThreads, smem_bytes(0, seg_rows), stream>>>(tasks, item_task, item_lo, item_end, counter, status,
-                                                            seg_rows);
+    const auto fn = kDrains[gf16 ? 1 : 0][drain_index(shape)];
+    fn<<<grid, kThreads, smem_bytes(gf16, seg_rows), stream>>>(tasks, item_task, item_lo, item_end, counter, status,
+                                                                 seg_rows);
     return cudaGetLastError();
 }
 

@@ -105,8 +105,7 @@ def device_stripes(torch, oracle, specs, rng):
         p = oracle.resolve(engine, k, m, L)
         data = rng.integers(0, 256, k * L, dtype=np.uint8)
         if op == OP_ENCODE:
-            exp = np.zeros(m * L, np.uint8)
-            oracle.batch_encoder(p).encode_into(data, exp)
+            exp = np.concatenate(encode_word(oracle, p, data)[k:])  # tower: k in-order feeds
             d_in = torch.from_numpy(data).cuda()
             d_out = torch.zeros(m * L, dtype=torch.uint8, device="cuda")
             stripes.append(Stripe(op, engine, k, m, L, d_in.data_ptr(), d_out.data_ptr()))

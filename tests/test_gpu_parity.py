@@ -315,6 +315,44 @@ def test_stripe_batch_matches_oracle(gpu, oracle):
     assert b.last_launches == 2  # plan + persistent drain
 
 
+def test_stripe_batch_with_tower_stripes(gpu, oracle):
+    """Tower stripes in the same batch as GF(256) stripes (each field through
+    its own plan launch and persistent drain): encodes equal the oracle's k
+    in-order feeds, decodes the data, in persistent, graph and plain modes;
+    tower stripes of more inputs than one staged segment (16 rows), odd
+    group counts and zero erasures among them.  Host-buffer batches refuse
+    tower stripes."""
+    torch = pytest.importorskip("torch")
+    from scrs_b200.api import RuntimeFailure
+    from scrs_b200.batch import OP_DECODE, OP_ENCODE, StripeBatch
+
+    specs, rng = make_mixed_batch(torch, 24, 21, lens=(1024, 4096, 1000, 64), kmax=40, mmax=12)
+    tower = [(32, 8, 4096), (8, 4, 1000), (300, 20, 130), (64, 32, 66), (17, 3, 2048), (2, 1, 4)]
+    for q, (k, m, L) in enumerate(tower):
+        specs.insert(3 * q + 1, (OP_ENCODE, Engine.TOWER, k, m, L))
+        specs.insert(3 * q + 2, (OP_DECODE, Engine.TOWER, k, m, L))
+    stripes, outs, expect, keep = device_stripes(torch, oracle, specs, rng)
+    b = StripeBatch(gpu.lib, len(stripes))
+    b.set(stripes)
+    for mode in ("persistent", "graph", "plain", "graph"):
+        for o in outs:
+            o.zero_()
+        if mode == "plain":
+            b.run_plain()
+        else:
+            b.run(graph=(mode == "graph"))
+        torch.cuda.synchronize()
+        b.check()
+        for q, (o, exp) in enumerate(zip(outs, expect)):
+            assert np.array_equal(o.cpu().numpy(), exp), (mode, specs[q])
+    assert b.last_launches == 4  # a plan launch and a persistent drain per field
+    h = torch.zeros(64, dtype=torch.uint8).pin_memory()
+    with pytest.raises(RuntimeFailure):
+        b.set_arrays(np.array([OP_ENCODE]), np.array([int(Engine.TOWER)]), np.array([2]), np.array([1]),
+                     np.array([32]), np.array([h.data_ptr()], dtype=np.uint64),
+                     np.array([h.data_ptr() + 32], dtype=np.uint64), host=True)
+
+
 def test_stripe_batch_host_buffers_pipelined(gpu, oracle):
     """Host-buffer batches run in up to 16 pieces whose copies overlap the
     compute; a decode stripe's present rows are copied on the host and only
