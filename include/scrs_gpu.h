@@ -369,7 +369,10 @@ typedef struct scrs_stripe_desc {
     /* encode: k*symbol_len data, row i at in + i*symbol_len.
      * decode: k received symbols, row i at in + i*symbol_len. */
     const uint8_t* in;
-    /* encode: m*symbol_len repairs.  decode: k*symbol_len data. */
+    /* encode: m*symbol_len repairs.  decode: k*symbol_len data.  The
+     * stripes' outputs must not overlap one another or any input: a stripe
+     * with more inputs than one staged segment accumulates partial sums in
+     * its output. */
     uint8_t* out;
     /* decode only: k codeword indices of the received rows (host memory). */
     const uint16_t* indices;
@@ -550,7 +553,8 @@ SCRS_API void scrs_server_destroy(scrs_server* server);
 /* Validates (profile, decode indices, budget: SCRS_ERR_CAPACITY when the
  * request alone exceeds it), queues, and admits what fits.  Buffers must
  * stay valid until the request's completion is returned; `out` is complete
- * on the device when it is.  The input is read after the work enqueued on
+ * on the device when it is.  Requests in flight at the same time must not
+ * share an output buffer (they may be coalesced into one stripe batch).  The input is read after the work enqueued on
  * req->stream before this call. */
 SCRS_API int32_t scrs_server_submit(scrs_server* server, const scrs_request* req,
                                     uint64_t* ticket, scrs_error* err);
