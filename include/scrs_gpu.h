@@ -516,8 +516,9 @@ SCRS_API void scrs_tune_table_clear(void);
  * of every engine are submitted with device-resident inputs and outputs and
  * admitted first come, first served as one of `slots` streams and the device
  * memory budget free up; admitted work overlaps on the device.  Waiting
- * GF(256) and tower requests are coalesced into one stripe batch per slot;
- * additive-FFT requests take a slot each and use engines kept resident per
+ * GF(256) requests and tower requests of at most 64 inputs and 32 outputs
+ * are coalesced into one stripe batch per slot; additive-FFT requests and
+ * larger tower requests take a slot each and use engines kept resident per
  * slot (least recently used profiles are evicted).  The budget counts every
  * admitted request's input and output bytes plus estimated resident engine
  * workspaces.  Results are identical to running each request alone. */
@@ -563,13 +564,13 @@ SCRS_API int32_t scrs_server_submit(scrs_server* server, const scrs_request* req
 SCRS_API int32_t scrs_server_progress(scrs_server* server, scrs_completion* done,
                                       uint32_t capacity, uint32_t* n_done,
                                       scrs_error* err);
-/* Build the resident engines of one additive-FFT profile for `op`
+/* Build the resident engines of one additive-FFT or large tower profile for `op`
  * on every slot, so that no request of that profile pays the build (device
  * allocations, which stall the whole device) on its way through.  For
  * start-up: SCRS_ERR_BAD_ARGUMENT (a = 3) while any slot is running
  * requests, (a = 1) for a GF(256) engine (its stripe batches need no
- * resident engines); SCRS_OK with nothing built for a tower profile (tower
- * requests run in the stripe batches too).  Resident engines count against
+ * resident engines); SCRS_OK with nothing built for a tower profile of at
+ * most 64 inputs and 32 outputs (those run in the stripe batches too).  Resident engines count against
  * the memory budget and
  * each slot keeps at most 8 profiles, least recently used evicted first. */
 SCRS_API int32_t scrs_server_reserve(scrs_server* server, int32_t op, int32_t engine,

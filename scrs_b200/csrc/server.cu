@@ -3,10 +3,10 @@
 //
 // Requests are submitted with device-resident inputs and outputs and admitted
 // as slots and device memory free up: each slot is a stream with its own
-// resident engines, so admitted work overlaps on the device.  GF(256) and
-// tower requests waiting in the queue are coalesced into one stripe batch
-// (plan launches + one persistent drain per field) per slot; additive-FFT
-// requests take a slot each.  Admission is first-come first-served under a device-memory budget
+// resident engines, so admitted work overlaps on the device.  GF(256)
+// requests and small tower requests waiting in the queue are coalesced into
+// one stripe batch (plan launches + one persistent drain per field) per slot;
+// additive-FFT requests and large tower requests take a slot each.  Admission is first-come first-served under a device-memory budget
 // that counts each admitted request's input and output bytes plus the
 // resident engines' workspaces.  progress() polls the slots' completion
 // events, returns finished requests and admits waiting ones; it never blocks
@@ -43,17 +43,25 @@ bool is_gf256(int32_t engine) {
     return engine == SCRS_ENGINE_STANDARD_CAUCHY || engine == SCRS_ENGINE_GOOD_CAUCHY;
 }
 
-// Requests that run as stripes of the slot's stripe batch (GF(256) and tower
-// multiply-XOR work); additive-FFT requests take a slot and resident engines.
-bool batchable(int32_t engine) { return is_gf256(engine) || engine == SCRS_ENGINE_TOWER; }
+// Requests that run as stripes of the slot's stripe batch: GF(256) requests,
+// and tower requests whose work per 2 KiB column chunk is bounded (at most 64
+// inputs and 32 outputs: the persistent drain gives one CTA a whole chunk).
+// Larger tower requests and additive-FFT requests take a slot each and use
+// resident engines (a large tower request's multiply then splits its inputs
+// over CTAs).
+constexpr uint64_t kTowerBatchMaxK = 64, kTowerBatchMaxM = 32;
+bool batchable(int32_t engine, uint64_t k, uint64_t m) {
+    return is_gf256(engine) || (engine == SCRS_ENGINE_TOWER && k <= kTowerBatchMaxK && m <= kTowerBatchMaxM);
+}
 
 // Engines of one profile, resident on one slot.
 struct Resident {
     scrs_profile p{};
-    scrs_batch_encoder* enc = nullptr;
+    scrs_batch_encoder* enc = nullptr;  // AFFT
     scrs_encode_scratch* enc_s = nullptr;
-    scrs_batch_decoder* dec = nullptr;
+    scrs_batch_decoder* dec = nullptr;  // tower, AFFT
     scrs_batch_decode_scratch* dec_s = nullptr;
+    DevBuf tower_coef;                  // tower encode: uint16[k*m]
     uint64_t bytes = 0;                 // estimated device footprint
     uint64_t last_use = 0;
     ~Resident() {
@@ -64,11 +72,11 @@ struct Resident {
     }
 };
 
-// Estimated device bytes of the additive-FFT engines a request needs
-// (admission only): two bit-sliced work arrays of ts rows plus per-point tables.
+// Estimated device bytes of the engines a request needs (admission only).
 uint64_t resident_estimate(const scrs_profile& p, int32_t op) {
-    (void)op;
     const uint64_t k = p.k, m = p.m, L = p.symbol_len;
+    if (p.engine == SCRS_ENGINE_TOWER) return op == SCRS_OP_ENCODE ? 2 * k * m : (k + m) * L + 4 * k * m + 64 * k;
+    // AFFT: two bit-sliced work arrays of ts rows plus per-point tables
     uint64_t ts = 1;
     while (ts < k + m) ts <<= 1;
     return 2 * ts * ((L + 63) / 64) * 64 + 32 * ts;
@@ -87,6 +95,7 @@ struct Req {
 struct Slot {
     OwnedStream stream;
     cudaEvent_t done = nullptr;
+    StatusWord status;                 // direct launches (large tower encodes)
     scrs_stripe_batch* batch = nullptr;
     std::map<ProfileKey, std::unique_ptr<Resident>> cache;
     uint64_t cache_bytes = 0;
@@ -155,7 +164,8 @@ int32_t resident(scrs_server* s, Slot& sl, const scrs_profile& p, int32_t op, Re
     auto it = sl.cache.find(key);
     Resident* R = it == sl.cache.end() ? nullptr : it->second.get();
     const bool need_enc = op == SCRS_OP_ENCODE, need_dec = op == SCRS_OP_DECODE;
-    const bool have = R && (need_enc ? R->enc != nullptr : R->dec != nullptr);
+    const bool have = R && (need_enc ? (p.engine == SCRS_ENGINE_TOWER ? R->tower_coef.p != nullptr : R->enc != nullptr)
+                                     : R->dec != nullptr);
     if (!have) {
         const uint64_t add = resident_estimate(p, op);
         while (!sl.cache.empty() && (sl.cache.size() >= kCachePerSlot || s->in_use + total_cache(s) + add > s->budget)) {
@@ -176,7 +186,13 @@ int32_t resident(scrs_server* s, Slot& sl, const scrs_profile& p, int32_t op, Re
             sl.cache[key] = std::move(nr);
         }
         int32_t rc = SCRS_OK;
-        if (need_enc) {
+        if (need_enc && p.engine == SCRS_ENGINE_TOWER) {
+            std::vector<uint16_t> pw(p.k + p.m), c(p.k * p.m);
+            hf::tower_powers((uint32_t)(p.k + p.m), pw.data());
+            hf::tower_coefficients((uint32_t)p.k, (uint32_t)p.m, pw.data(), c.data());
+            SCRS_CUDA(R->tower_coef.ensure(c.size() * 2));
+            SCRS_CUDA(upload_now(R->tower_coef.p, c.data(), c.size() * 2, sl.stream.s));
+        } else if (need_enc) {
             rc = scrs_batch_encoder_create(&p, &R->enc, err);
             if (!rc) rc = scrs_batch_encoder_scratch(R->enc, &R->enc_s, err);
         } else {
@@ -195,7 +211,7 @@ int32_t resident(scrs_server* s, Slot& sl, const scrs_profile& p, int32_t op, Re
     return SCRS_OK;
 }
 
-// Enqueue one additive-FFT request on the slot's stream.
+// Enqueue one large tower or additive-FFT request on the slot's stream.
 int32_t launch_single(scrs_server* s, Slot& sl, Req& r, scrs_error* err) {
     scrs_profile p{};
     int32_t rc = scrs_profile_resolve(r.d.engine, r.d.k, r.d.m, r.d.symbol_len, &p, err);
@@ -205,6 +221,24 @@ int32_t launch_single(scrs_server* s, Slot& sl, Req& r, scrs_error* err) {
     if (rc) return rc;
     const uint64_t k = p.k, m = p.m, L = p.symbol_len;
     cudaStream_t st = sl.stream.s;
+    if (r.d.op == SCRS_OP_ENCODE && p.engine == SCRS_ENGINE_TOWER) {
+        // Block encode of all k rows: repairs = C^T * data over GF((2^8)^2)
+        // (the incremental tower encode of k in-order feeds, tower/encoder.rs:89-116).
+        MxkTask T{};
+        T.in = r.d.in;
+        T.out = r.d.out;
+        T.coef = R->tower_coef.p;
+        T.L = L;
+        T.in_stride = L;
+        T.out_stride = L;
+        T.n_in = (uint32_t)k;
+        T.n_out = (uint32_t)m;
+        T.ld = (uint32_t)m;
+        T.n_items = n_chunks(L, true);
+        T.aligned = (L % 16 == 0 && aligned16(r.d.in) && aligned16(r.d.out)) ? 1u : 0u;
+        SCRS_CUDA(launch_mxk_single(T, 1, sl.status.dev, 0, st));
+        return SCRS_OK;
+    }
     sl.used.push_back(R);
     if (r.d.op == SCRS_OP_ENCODE)
         return scrs_batch_encode_into_with_device(R->enc, r.d.in, k * L, r.d.out, m * L, R->enc_s, st, err);
@@ -248,6 +282,7 @@ void retire(scrs_server* s, Slot& sl, uint64_t t_done) {
         if (R->enc) status = internal_batch_encoder_status(R->enc, &e);
         if (!status && R->dec) status = internal_batch_decoder_status(R->dec, &e);
     }
+    if (!status) status = take_status(sl.status, &e);
     for (const Req& r : sl.running) {
         finish(s, r, status, t_done);
         s->free_events.push_back(r.ready);  // its wait has run: reusable
@@ -286,7 +321,7 @@ void admit(scrs_server* s) {
         Req& head = s->queue.front();
         if (s->in_use + head.bytes > s->budget) return;  // wait for memory
         Slot* pick = nullptr;
-        const bool batch = batchable(head.d.engine);
+        const bool batch = batchable(head.d.engine, head.d.k, head.d.m);
         for (auto& slp : s->slots) {
             if (slp->busy) continue;
             if (!pick) pick = slp.get();
@@ -304,7 +339,7 @@ void admit(scrs_server* s) {
         if (batch) {
             // coalesce every waiting GF(256) and tower request that fits, in arrival order
             for (auto it = s->queue.begin(); it != s->queue.end() && group.size() < kMaxCoalesce;) {
-                if (!batchable(it->d.engine)) {
+                if (!batchable(it->d.engine, it->d.k, it->d.m)) {
                     ++it;
                     continue;
                 }
@@ -350,6 +385,7 @@ extern "C" int32_t scrs_server_create(uint64_t memory_budget, uint32_t n_slots, 
         std::unique_ptr<Slot> sl(new (std::nothrow) Slot());
         if (!sl) return set_err(err, SCRS_ERR_OUT_OF_MEMORY, sizeof(Slot));
         SCRS_CUDA(sl->stream.init());
+        SCRS_CUDA(sl->status.init());
         SCRS_CUDA(cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming));
         s->slots.push_back(std::move(sl));
     }
@@ -390,7 +426,7 @@ extern "C" int32_t scrs_server_submit(scrs_server* s, const scrs_request* rq, ui
         }
     }
     r.bytes = k * L + (rq->op == SCRS_OP_ENCODE ? m : k) * L;
-    const uint64_t need = r.bytes + (batchable(p.engine) ? 0 : resident_estimate(p, rq->op));
+    const uint64_t need = r.bytes + (batchable(p.engine, p.k, p.m) ? 0 : resident_estimate(p, rq->op));
     if (need > s->budget) return set_err(err, SCRS_ERR_CAPACITY, need, s->budget);
     if (s->free_events.empty()) {
         cudaEvent_t e = nullptr;
@@ -439,7 +475,7 @@ extern "C" int32_t scrs_server_reserve(scrs_server* s, int32_t op, int32_t engin
     for (auto& sl : s->slots)  // engines in use must not be evicted
         if (sl->busy) return set_err(err, SCRS_ERR_BAD_ARGUMENT, 3);
     if (is_gf256(p.engine)) return set_err(err, SCRS_ERR_BAD_ARGUMENT, 1);
-    if (p.engine == SCRS_ENGINE_TOWER) return set_err(err, SCRS_OK);  // runs in the stripe batch: nothing to build
+    if (batchable(p.engine, p.k, p.m)) return set_err(err, SCRS_OK);  // runs in the stripe batch: nothing to build
     for (auto& sl : s->slots) {
         Resident* R = nullptr;
         rc = resident(s, *sl, p, op, &R, err);
