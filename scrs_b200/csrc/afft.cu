@@ -347,13 +347,20 @@ struct PassIo {
 
 // acc ^= f * x for every lane of the calling warp (all 32 lanes call it
 // together; a lane with nothing to multiply passes f = 0), each lane with its
-// own factor: the warp's distinct factors are served one at a time, every
-// group through the uniform jump table (brx.idx.uni is valid there: all
-// active lanes share the index).  A warp whose lanes share one factor makes
-// one pass.
+// own factor.  A warp whose lanes hold one or two distinct factors serves
+// them one at a time, every group through the uniform jump table (brx.idx.uni
+// is valid there: all active lanes share the index); with more, every lane
+// runs the branch-free product (mul16_masked), whose cost does not grow with
+// the number of factors.
 __device__ __forceinline__ void mul16_lanes(uint32_t f, uint32_t (&acc)[16], const uint32_t (&x)[16]) {
-    unsigned left = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
+    const unsigned same = __match_any_sync(0xFFFFFFFFu, f);
+    const unsigned leaders = __ballot_sync(0xFFFFFFFFu, (unsigned)(__ffs(same) - 1) == (unsigned)lane);
+    if (__popc(leaders) > 2) {
+        if (f) mul16_masked(f, acc, x);
+        return;
+    }
+    unsigned left = 0xFFFFFFFFu;
     while (left) {
         const uint32_t fl = __shfl_sync(0xFFFFFFFFu, f, __ffs(left) - 1);
         const bool mine = ((left >> lane) & 1u) && f == fl;
@@ -421,27 +428,40 @@ __global__ void __launch_bounds__(kTileThreads) afft_tile_kernel(uint8_t* work, 
             const uint32_t q = x & 3, g = (x >> 2) % gn, i = (x >> 2) / gn;
             cp_async_16(piece(i, q, g), work + ((uint64_t)row_of(i) * G + g0 + g) * 64 + 16 * q);
         }
-        cp_async_wait_all();
     }
+    // The node factors of the pass, after the tile: at tile level lam the rows
+    // whose level bits above the pair bit read u share factor
+    // factors[(root << l) + (hi << lam) + u]; entry (1 << lam) - 1 + u of the
+    // phase's table, 2^c - 1 entries per phase.
+    uint16_t* fac = reinterpret_cast<uint16_t*>(tile + (size_t)rows * gt * 64);
+    const uint32_t per_phase = (1u << c) - 1u;
+    for (uint32_t x = tid; x < (uint32_t)ph.n * per_phase; x += blockDim.x) {
+        const uint32_t p = x / per_phase, at = x - p * per_phase;
+        const int lam = 31 - __clz(at + 1);
+        const uint32_t u = at + 1 - (1u << lam);
+        fac[x] = factors[((uint64_t)ph.root[p] << (l0 + lam)) + ((uint64_t)hi << lam) + u];
+    }
+    if (!slice) cp_async_wait_all();
     __syncthreads();
     const uint32_t items = (rows / 2) * gn;
+    const bool gpow = (gn & (gn - 1u)) == 0;  // the column split by shift and mask
+    const int gsh = __ffs(gn) - 1;
     for (int p = 0; p < ph.n; p++) {
-        const uint32_t root = ph.root[p];
         const bool fwd = ph.forward[p] != 0;
         for (int s = 0; s < c; s++) {
             const int lam = fwd ? s : c - 1 - s;  // tile-local level
-            const int l = l0 + lam;
             const int b = c - 1 - lam;            // pair bit among the level bits
+            const uint16_t* lf = fac + p * per_phase + (1u << lam) - 1u;
             for (uint32_t x0 = tid - lane; x0 < items; x0 += blockDim.x) {
                 const uint32_t x = x0 + lane;
                 const bool valid = x < items;
-                const uint32_t g = valid ? x % gn : 0u;
-                uint32_t r = valid ? x / gn : 0u;
+                const uint32_t g = !valid ? 0u : gpow ? (x & (gn - 1u)) : x % gn;
+                uint32_t r = !valid ? 0u : gpow ? (x >> gsh) : x / gn;
                 const uint32_t low = r & low_mask;
                 r >>= e;
                 const uint32_t lev_lo = ((r >> b) << (b + 1)) | (r & ((1u << b) - 1u));
                 const uint32_t ilo = (lev_lo << e) | low, ihi = ilo | (1u << (b + e));
-                const uint32_t f = valid ? factors[(root << l) + (row_of(ilo) >> (D - l))] : 0u;
+                const uint32_t f = valid ? lf[r >> b] : 0u;
                 uint32_t wl[16], wh[16];
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
@@ -555,11 +575,15 @@ std::vector<PassPlan> plan_passes(int D, uint32_t gt) {
     return out;
 }
 
+// Shared memory after the tile: the node factors of up to two phases of a
+// pass of at most 10 levels (2 * (2^10 - 1) uint16).
+constexpr size_t kFactorSmem = 2 * 1024 * 2;
+
 cudaError_t set_tile_attr() {
     static std::atomic<uint64_t> attr{0};
     return once_per_device(attr, [] {
         return cudaFuncSetAttribute(afft_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(kTileElems * 64));
+                                    (int)(kTileElems * 64 + kFactorSmem));
     });
 }
 
@@ -567,9 +591,12 @@ cudaError_t launch_pass(uint8_t* work, uint32_t G, int D, const PassPlan& P, uin
                         const uint16_t* factors, const PassIo& io, int slice, int unslice, cudaStream_t st) {
     const uint32_t col_tiles = (G + gt - 1) / gt;
     const uint32_t tiles = (1u << (D - P.c - P.e)) * col_tiles;
-    const size_t smem = ((size_t)1 << (P.c + P.e)) * gt * 64;
-    afft_tile_kernel<<<tiles, kTileThreads, smem, st>>>(work, G, D, P.l0, P.c, P.e, gt, ph, factors, io, slice,
-                                                        unslice);
+    const size_t rows = (size_t)1 << (P.c + P.e);
+    const size_t smem = rows * gt * 64 + (size_t)std::max(ph.n, 1) * (((size_t)1 << P.c) - 1) * 2;
+    // one butterfly per thread and level: a multiple of 32 threads, at most kTileThreads
+    const uint32_t bfly = (uint32_t)(rows / 2) * gt;
+    const int threads = (int)std::min<uint32_t>(kTileThreads, std::max<uint32_t>(32, (bfly + 31) / 32 * 32));
+    afft_tile_kernel<<<tiles, threads, smem, st>>>(work, G, D, P.l0, P.c, P.e, gt, ph, factors, io, slice, unslice);
     return cudaGetLastError();
 }
 

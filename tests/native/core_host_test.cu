@@ -72,10 +72,18 @@ int main() {
         memcpy(p, x, sizeof p);
         bitslice16(p);
         bitslice16(acc);
+        uint32_t acc2[16];
+        memcpy(acc2, acc, sizeof acc2);
         mul16(c, acc, p);
         bitslice16(acc);
         if (memcmp(acc, expect, 64)) {
             if (failures < 10) printf("mul16 mismatch c=%04x\n", c);
+            failures++;
+        }
+        mul16_masked(c, acc2, p);  // the branch-free form
+        bitslice16(acc2);
+        if (memcmp(acc2, expect, 64)) {
+            if (failures < 10) printf("mul16_masked mismatch c=%04x\n", c);
             failures++;
         }
         // plane layout: w[s] = bit s of component a, w[8+s] = bit s of b.
