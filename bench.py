@@ -1151,6 +1151,9 @@ def run_ours(args, world, rank, local):
             "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if
             peak_kind == "measured" else "fallback 6650 GB/s",
             "traffic": round(ratio * algorithmic_bytes()) if ratio else None,
+            "traffic_source": ("DRAM bytes per algorithmic byte of an ncu capture at 8192+8192 stripes "
+                               "(profiles/gf256_mxk_cfg1_ncu.md) times this launch's algorithmic bytes: the "
+                               "full-size launch is too large to capture; traffic grows with the stripes"),
             "kernel": ("persistent drain: scrs_spec_drain (encode stripes, kernel specialised to the matrix) "
                        "then mxk_kernel<0, 7> (decode stripes; rows 16-byte aligned, whole 2 KiB chunks, "
                        "one segment)" if enc_spec else "mxk_kernel<0, 7> persistent drain"),
