@@ -1203,7 +1203,7 @@ def run_ours(args, world, rank, local):
                                       "stripe), so e2e cannot exceed the host-to-device copy rate measured alone "
                                       "(1 GiB pinned copy, CUDA events)"},
                "path": "scrs_stripe_batch_set_host + scrs_stripe_batch_run (pinned host buffers; copies of "
-                       "16 pieces overlap the compute, both copy directions at once; decode stripes copy back "
+                       "32 pieces overlap the compute, both copy directions at once; decode stripes copy back "
                        "only their missing rows, their present rows are copied host-side while the GPU runs)"}
         launches += hb.last_launches * n_e2e
     extras = {}
