@@ -46,6 +46,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "encode/decode GB/s and HBM-roofline % on 1 B200; batched vs plain; p50/p99 ms"
 K, M, L = 10, 4, 4096
 STRIPES = 65536
+MIXED_STRIPES = 8192  # stripes of the mixed batch; smaller values are for ncu captures
 SEED = 0x5C250001
 
 
@@ -447,7 +448,7 @@ def extra_mixed(torch, api, cpu=None):
     from scrs_b200.batch import DESC_DTYPE, OP_DECODE, OP_ENCODE, StripeBatch
 
     rng = np.random.default_rng(SEED + 4)
-    n = 8192
+    n = MIXED_STRIPES
     ks = rng.integers(4, 65, n)
     ms = rng.integers(1, 17, n)
     Ls = rng.choice([1024, 4096, 65536], n)
@@ -537,7 +538,7 @@ def extra_mixed(torch, api, cpu=None):
                         cpu.api.batch_encoder(p).encode_into(word[:k].reshape(-1), exp)
                     ok &= bool(np.array_equal(got, exp))
                     checked += 1
-    res = {"workload": "8192 stripes, k~U[4,64], m~U[1,16], L in {1,4,64} KiB, Standard/Good mixed, half encode "
+    res = {"workload": f"{n} stripes, k~U[4,64], m~U[1,16], L in {{1,4,64}} KiB, Standard/Good mixed, half encode "
                        "half decode of real codewords (random erasures <= m)",
            "persistent_graph_GBps": round(goodput / t_graph / 1e6, 1),
            "plain_per_stripe_GBps": round(goodput / t_plain / 1e6, 1),
@@ -1262,7 +1263,7 @@ def run_reference(args, world, rank):
 
 
 def main():
-    global STRIPES
+    global STRIPES, MIXED_STRIPES
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
@@ -1273,10 +1274,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg (profiling runs)")
     ap.add_argument("--stripes", type=int, default=STRIPES,
                     help="stripes per op per GPU; the headline uses 65536, smaller values are for ncu captures")
+    ap.add_argument("--mixed-stripes", type=int, default=MIXED_STRIPES,
+                    help="stripes of the mixed batch extra; the reported figure uses 8192, smaller values are for ncu "
+                         "captures")
     ap.add_argument("--only", choices=sorted(EXTRAS),
                     help="run just one of the extras and print its JSON (profiling runs; no headline line)")
     args = ap.parse_args()
     STRIPES = args.stripes
+    MIXED_STRIPES = args.mixed_stripes
     if args.only:
         import torch
         import scrs_b200

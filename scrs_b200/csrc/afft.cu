@@ -5,7 +5,8 @@
 // Rows between stages are kept bit-sliced in HBM: a row of L bytes is stored
 // as G = ceil(L/64) groups of 64 bytes, each group the 16 bit planes of 32
 // field elements (scrs_b200/csrc/common.cuh bitslice16).  Bytes are sliced
-// once on the way in (scale_in) and unsliced once on the way out (scale_out).
+// once on the way in (the first transform pass) and unsliced once on the way
+// out (the last).
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -115,89 +116,176 @@ __device__ __forceinline__ uint32_t add_mod(uint32_t a, uint32_t b) {
 }
 __device__ __forceinline__ uint32_t sub_mod(uint32_t a, uint32_t b) { return a >= b ? a - b : a + kMult - b; }
 
-// Walsh-Hadamard butterflies over index bits [lo, lo + nb) (decoder.rs:732-755);
-// one CTA per group of 2^nb elements that differ only in those bits.
-__global__ void __launch_bounds__(1024) wht_pass_kernel(uint32_t* v, uint32_t ts, int lo, int nb) {
+// ---- erasure locator (decoder.rs:672-755) ----------------------------------------
+// log L(x) for every point x is a Walsh-Hadamard transform (mod 65535) of the
+// product of two transforms: one of the erasure indicator, one of the
+// logarithm table's first ts entries.  The second depends on ts alone, so the
+// codec computes it once (log_walsh_host), with the final transform's 1/ts
+// folded in; a decode runs two transforms.  Every level of a Walsh-Hadamard
+// transform is exact arithmetic mod 65535 and the levels commute, so any
+// grouping of levels into rounds gives the reference's residues.
+//
+// In one CTA (ts <= kLocatorOneCtaTs): round A takes index bits [0, 5 + R2)
+// per warp, bits 0-4 across the lanes (shuffles) and bits 5.. through
+// registers; round B takes the remaining RB <= 5 bits through registers,
+// consecutive threads on consecutive entries (no bank conflicts).  The
+// indicator is read straight from the known-point mask, the product with the
+// log transform happens on the first transform's last store, and the
+// second's last store writes values and derivatives.
+constexpr uint32_t kLocatorOneCtaTs = 16384;
+// Round A of a 2^14 transform has 32 blocks of 512 entries, round B 512
+// groups: 16 warps serve both without idle threads.
+constexpr int kLocatorThreads = 512;
+
+template <int R2, class Load, class Store>
+__device__ __forceinline__ void wht_round_lanes(int D, Load load, Store store) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t ts = 1u << D;
+    const int lane_bits = D < 5 ? D : 5;
+    const uint32_t span = 32u << R2;
+    const uint32_t nblk = ts > span ? ts / span : 1u;
+    for (uint32_t b = warp; b < nblk; b += nwarps) {
+        uint32_t x[1 << R2];
+#pragma unroll
+        for (int j = 0; j < (1 << R2); j++) {
+            const uint32_t idx = b * span + 32u * j + lane;
+            x[j] = idx < ts ? load(idx) : 0u;
+        }
+#pragma unroll
+        for (int s = 0; s < R2; s++)
+#pragma unroll
+            for (int j = 0; j < (1 << R2); j++)
+                if (!(j & (1 << s))) {
+                    const uint32_t a = x[j], c = x[j | (1 << s)];
+                    x[j] = add_mod(a, c);
+                    x[j | (1 << s)] = sub_mod(a, c);
+                }
+        for (int s = 0; s < lane_bits; s++) {
+            const bool upper = (lane >> s) & 1u;
+#pragma unroll
+            for (int j = 0; j < (1 << R2); j++) {
+                const uint32_t y = __shfl_xor_sync(0xFFFFFFFFu, x[j], 1u << s);
+                x[j] = upper ? sub_mod(y, x[j]) : add_mod(x[j], y);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < (1 << R2); j++) {
+            const uint32_t idx = b * span + 32u * j + lane;
+            if (idx < ts) store(idx, x[j]);
+        }
+    }
+}
+
+template <int RB, class Load, class Store>
+__device__ __forceinline__ void wht_round_regs(int D, int lo, Load load, Store store) {
+    const uint32_t groups = 1u << (D - RB);
+    for (uint32_t g = threadIdx.x; g < groups; g += blockDim.x) {
+        const uint32_t base = ((g >> lo) << (lo + RB)) | (g & ((1u << lo) - 1u));
+        uint32_t x[1 << RB];
+#pragma unroll
+        for (int j = 0; j < (1 << RB); j++) x[j] = load(base + ((uint32_t)j << lo));
+#pragma unroll
+        for (int s = 0; s < RB; s++)
+#pragma unroll
+            for (int j = 0; j < (1 << RB); j++)
+                if (!(j & (1 << s))) {
+                    const uint32_t a = x[j], c = x[j | (1 << s)];
+                    x[j] = add_mod(a, c);
+                    x[j | (1 << s)] = sub_mod(a, c);
+                }
+#pragma unroll
+        for (int j = 0; j < (1 << RB); j++) store(base + ((uint32_t)j << lo), x[j]);
+    }
+}
+
+template <int R2, int RB>
+__device__ void locator_cta(const uint8_t* known, int D, const uint32_t* lw, const uint16_t* exp16,
+                            uint16_t* values, uint16_t* derivs, uint32_t* v) {
+    auto indicator = [&](uint32_t i) -> uint32_t { return known[i] ? 0u : 1u; };
+    auto ld = [&](uint32_t i) -> uint32_t { return v[i]; };
+    auto st = [&](uint32_t i, uint32_t x) { v[i] = x; };
+    auto st_mul = [&](uint32_t i, uint32_t x) { v[i] = (uint32_t)(((uint64_t)x * lw[i]) % kMult); };
+    auto st_out = [&](uint32_t i, uint32_t x) {
+        const uint16_t prod = exp16[x];
+        const bool have = known[i] != 0;
+        values[i] = have ? prod : 0;
+        derivs[i] = have ? 0 : prod;
+    };
+    if constexpr (RB == 0) {
+        wht_round_lanes<R2>(D, indicator, st_mul);
+        __syncthreads();
+        wht_round_lanes<R2>(D, ld, st_out);
+    } else {
+        wht_round_lanes<R2>(D, indicator, st);
+        __syncthreads();
+        wht_round_regs<RB>(D, 5 + R2, ld, st_mul);
+        __syncthreads();
+        wht_round_lanes<R2>(D, ld, st);
+        __syncthreads();
+        wht_round_regs<RB>(D, 5 + R2, ld, st_out);
+    }
+}
+
+__global__ void __launch_bounds__(kLocatorThreads) locator_one_cta_kernel(const uint8_t* known, int D, const uint32_t* lw,
+                                                               const uint16_t* exp16, uint16_t* values,
+                                                               uint16_t* derivs) {
+    extern __shared__ uint32_t sm_loc[];
+    const int r2 = D <= 5 ? 0 : min(4, D - 5);
+    const int rb = D <= 9 ? 0 : D - 9;
+    switch (r2 * 8 + rb) {
+        case 0: locator_cta<0, 0>(known, D, lw, exp16, values, derivs, sm_loc); break;
+        case 8: locator_cta<1, 0>(known, D, lw, exp16, values, derivs, sm_loc); break;
+        case 16: locator_cta<2, 0>(known, D, lw, exp16, values, derivs, sm_loc); break;
+        case 24: locator_cta<3, 0>(known, D, lw, exp16, values, derivs, sm_loc); break;
+        case 32: locator_cta<4, 0>(known, D, lw, exp16, values, derivs, sm_loc); break;
+        case 33: locator_cta<4, 1>(known, D, lw, exp16, values, derivs, sm_loc); break;
+        case 34: locator_cta<4, 2>(known, D, lw, exp16, values, derivs, sm_loc); break;
+        case 35: locator_cta<4, 3>(known, D, lw, exp16, values, derivs, sm_loc); break;
+        case 36: locator_cta<4, 4>(known, D, lw, exp16, values, derivs, sm_loc); break;
+        case 37: locator_cta<4, 5>(known, D, lw, exp16, values, derivs, sm_loc); break;
+        default: break;  // D > 14 takes the multi-CTA path
+    }
+}
+
+// Larger transforms: passes over index bits [lo, lo + nb), one CTA per group
+// of 2^nb entries that differ only in those bits.  The first pass of the
+// first transform reads the indicator from the known-point mask (in_mode 1);
+// the last pass of the first transform multiplies by the log transform
+// (out_mode 1); the last pass of the second writes values and derivatives
+// (out_mode 2).
+__global__ void __launch_bounds__(1024) wht_pass_kernel(uint32_t* v, int lo, int nb, int in_mode, int out_mode,
+                                                        const uint8_t* known, const uint32_t* lw,
+                                                        const uint16_t* exp16, uint16_t* values, uint16_t* derivs) {
     extern __shared__ uint32_t sv[];
     const uint32_t gsize = 1u << nb;
     const uint32_t gidx = blockIdx.x;
     const uint32_t base = ((gidx >> lo) << (lo + nb)) | (gidx & ((1u << lo) - 1u));
-    for (uint32_t t = threadIdx.x; t < gsize; t += blockDim.x) sv[t] = v[base + ((size_t)t << lo)];
+    for (uint32_t t = threadIdx.x; t < gsize; t += blockDim.x) {
+        const uint32_t i = base + (t << lo);
+        sv[t] = in_mode ? (known[i] ? 0u : 1u) : v[i];
+    }
     __syncthreads();
-    for (uint32_t half = 1; half < gsize; half <<= 1) {
+    for (int s = 0; s < nb; s++) {
         for (uint32_t p = threadIdx.x; p < gsize / 2; p += blockDim.x) {
-            uint32_t i = ((p / half) * 2 * half) + (p % half);
-            uint32_t a = sv[i], b = sv[i + half];
-            sv[i] = add_mod(a, b);
-            sv[i + half] = sub_mod(a, b);
+            const uint32_t i = ((p >> s) << (s + 1)) | (p & ((1u << s) - 1u));
+            const uint32_t a = sv[i], c = sv[i + (1u << s)];
+            sv[i] = add_mod(a, c);
+            sv[i + (1u << s)] = sub_mod(a, c);
         }
         __syncthreads();
     }
-    for (uint32_t t = threadIdx.x; t < gsize; t += blockDim.x) v[base + ((size_t)t << lo)] = sv[t];
-}
-
-__global__ void locator_init_kernel(const uint8_t* known, uint32_t ts, const uint16_t* log16, uint32_t* a,
-                                    uint32_t* b) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ts; i += gridDim.x * blockDim.x) {
-        a[i] = known[i] ? 0u : 1u;
-        b[i] = log16[i];
-    }
-}
-
-__global__ void locator_mul_kernel(uint32_t* a, const uint32_t* b, uint32_t ts) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ts; i += gridDim.x * blockDim.x)
-        a[i] = (uint32_t)(((uint64_t)a[i] * b[i]) % kMult);
-}
-
-// The whole locator in one CTA for transforms of at most kLocatorOneCtaTs
-// points: the same steps as locator_init -> 2 WHTs -> locator_mul -> WHT ->
-// locator_finish, on shared-memory copies of both arrays (one launch instead
-// of nine; at these sizes launch gaps, not arithmetic, set the time).
-constexpr uint32_t kLocatorOneCtaTs = 16384;
-
-__device__ __forceinline__ void wht_block(uint32_t* v, uint32_t ts) {
-    for (uint32_t half = 1; half < ts; half <<= 1) {
-        for (uint32_t p = threadIdx.x; p < ts / 2; p += blockDim.x) {
-            const uint32_t i = ((p / half) * 2 * half) + (p % half);
-            const uint32_t a = v[i], b = v[i + half];
-            v[i] = add_mod(a, b);
-            v[i + half] = sub_mod(a, b);
+    for (uint32_t t = threadIdx.x; t < gsize; t += blockDim.x) {
+        const uint32_t i = base + (t << lo), x = sv[t];
+        if (out_mode == 0) {
+            v[i] = x;
+        } else if (out_mode == 1) {
+            v[i] = (uint32_t)(((uint64_t)x * lw[i]) % kMult);
+        } else {
+            const uint16_t prod = exp16[x];
+            const bool have = known[i] != 0;
+            values[i] = have ? prod : 0;
+            derivs[i] = have ? 0 : prod;
         }
-        __syncthreads();
-    }
-}
-
-__global__ void __launch_bounds__(1024) locator_one_cta_kernel(const uint8_t* known, uint32_t ts, uint32_t inv_size,
-                                                               const uint16_t* log16, const uint16_t* exp16,
-                                                               uint16_t* values, uint16_t* derivs) {
-    extern __shared__ uint32_t sm_loc[];
-    uint32_t* a = sm_loc;
-    uint32_t* b = sm_loc + ts;
-    for (uint32_t i = threadIdx.x; i < ts; i += blockDim.x) {
-        a[i] = known[i] ? 0u : 1u;
-        b[i] = log16[i];
-    }
-    __syncthreads();
-    wht_block(a, ts);
-    wht_block(b, ts);
-    for (uint32_t i = threadIdx.x; i < ts; i += blockDim.x) a[i] = (uint32_t)(((uint64_t)a[i] * b[i]) % kMult);
-    __syncthreads();
-    wht_block(a, ts);
-    for (uint32_t i = threadIdx.x; i < ts; i += blockDim.x) {
-        const uint32_t e = (uint32_t)(((uint64_t)a[i] * inv_size) % kMult);
-        const uint16_t prod = exp16[e];
-        values[i] = known[i] ? prod : 0;
-        derivs[i] = known[i] ? 0 : prod;
-    }
-}
-
-__global__ void locator_finish_kernel(const uint32_t* a, const uint8_t* known, uint32_t ts, uint32_t inv_size,
-                                      const uint16_t* exp16, uint16_t* values, uint16_t* derivs) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ts; i += gridDim.x * blockDim.x) {
-        uint32_t e = (uint32_t)(((uint64_t)a[i] * inv_size) % kMult);
-        uint16_t prod = exp16[e];
-        values[i] = known[i] ? prod : 0;
-        derivs[i] = known[i] ? 0 : prod;
     }
 }
 
@@ -673,36 +761,60 @@ uint32_t mod_pow(uint32_t base, uint32_t e) {
     return (uint32_t)r;
 }
 
-cudaError_t run_wht(uint32_t* v, uint32_t ts, int D, cudaStream_t st) {
+// One Walsh-Hadamard transform of v (2^D entries) as passes of at most 8
+// index bits, enough groups per pass to spread over the SMs; in_mode and
+// out_mode as wht_pass_kernel, applied on the first and last pass.
+cudaError_t run_wht(uint32_t* v, uint32_t ts, int D, int in_mode, int out_mode, const uint8_t* known,
+                    const uint32_t* lw, const uint16_t* exp16, uint16_t* values, uint16_t* derivs,
+                    cudaStream_t st) {
     static std::atomic<uint64_t> attr{0};
     cudaError_t ea = once_per_device(attr, [] {
         return cudaFuncSetAttribute(wht_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 4);
     });
     if (ea != cudaSuccess) return ea;
-    // passes of at most 8 index bits: enough groups per pass to spread over
-    // the SMs (one CTA per group of 2^nb elements)
-    std::vector<std::pair<int, int>> passes;
     const int n_pass = (D + 7) / 8;
     for (int q = 0, lo = 0; q < n_pass; q++) {
         const int nb = (D - lo + (n_pass - q) - 1) / (n_pass - q);
-        passes.push_back({lo, nb});
-        lo += nb;
-    }
-    for (auto& p : passes) {
-        uint32_t groups = ts >> p.second;
-        uint32_t gsize = 1u << p.second;
+        const uint32_t groups = ts >> nb, gsize = 1u << nb;
         wht_pass_kernel<<<groups, std::min<uint32_t>(1024, std::max<uint32_t>(32, gsize / 2)), gsize * 4, st>>>(
-            v, ts, p.first, p.second);
+            v, lo, nb, q == 0 ? in_mode : 0, q + 1 == n_pass ? out_mode : 0, known, lw, exp16, values, derivs);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
+        lo += nb;
     }
     return cudaSuccess;
 }
 
+// The logarithm table's first ts entries (log 0 = 0, as the device table),
+// Walsh-Hadamard transformed mod 65535 (decoder.rs:691-694), times the final
+// transform's 1/ts (decoder.rs:700-703).
+std::vector<uint32_t> log_walsh_host(uint32_t ts, int D) {
+    static const std::vector<uint32_t> lg = [] {
+        std::vector<uint32_t> t(65536, 0);
+        uint16_t v = 1;
+        for (uint32_t i = 0; i < kMult; i++) {
+            t[v] = i;
+            v = hf::mul16(v, hf::kGen16);
+        }
+        return t;
+    }();
+    std::vector<uint32_t> w(lg.begin(), lg.begin() + ts);
+    for (uint32_t h = 1; h < ts; h <<= 1)
+        for (uint32_t b = 0; b < ts; b += 2 * h)
+            for (uint32_t p = b; p < b + h; p++) {
+                const uint32_t a = w[p], c = w[p + h];
+                w[p] = a + c >= kMult ? a + c - kMult : a + c;
+                w[p + h] = a >= c ? a - c : a + kMult - c;
+            }
+    const uint64_t inv = mod_pow(32768, (uint32_t)D);
+    for (auto& e : w) e = (uint32_t)(e * inv % kMult);
+    return w;
+}
+
 }  // namespace
 
-int32_t afft_locator_device(const uint8_t* d_known, uint32_t ts, uint32_t* wa, uint32_t* wb, uint16_t* values,
-                            uint16_t* derivs, cudaStream_t st, scrs_error* err) {
+int32_t afft_locator_device(const uint8_t* d_known, uint32_t ts, const uint32_t* log_walsh, uint32_t* wa,
+                            uint16_t* values, uint16_t* derivs, cudaStream_t st, scrs_error* err) {
     const uint16_t *lg, *ex;
     SCRS_CUDA(log16_tables(&lg, &ex));
     int D = 0;
@@ -711,23 +823,15 @@ int32_t afft_locator_device(const uint8_t* d_known, uint32_t ts, uint32_t* wa, u
         static std::atomic<uint64_t> attr{0};
         SCRS_CUDA(once_per_device(attr, [] {
             return cudaFuncSetAttribute(locator_one_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)(2 * kLocatorOneCtaTs * sizeof(uint32_t)));
+                                        (int)(kLocatorOneCtaTs * sizeof(uint32_t)));
         }));
-        locator_one_cta_kernel<<<1, 1024, 2 * ts * sizeof(uint32_t), st>>>(d_known, ts, mod_pow(32768, (uint32_t)D),
-                                                                           lg, ex, values, derivs);
+        locator_one_cta_kernel<<<1, kLocatorThreads, ts * sizeof(uint32_t), st>>>(d_known, D, log_walsh, ex, values,
+                                                                                   derivs);
         SCRS_CUDA(cudaGetLastError());
         return SCRS_OK;
     }
-    const int g = grid_for(ts, 256);
-    locator_init_kernel<<<g, 256, 0, st>>>(d_known, ts, lg, wa, wb);
-    SCRS_CUDA(cudaGetLastError());
-    SCRS_CUDA(run_wht(wa, ts, D, st));
-    SCRS_CUDA(run_wht(wb, ts, D, st));
-    locator_mul_kernel<<<g, 256, 0, st>>>(wa, wb, ts);
-    SCRS_CUDA(cudaGetLastError());
-    SCRS_CUDA(run_wht(wa, ts, D, st));
-    locator_finish_kernel<<<g, 256, 0, st>>>(wa, d_known, ts, mod_pow(32768, (uint32_t)D), ex, values, derivs);
-    SCRS_CUDA(cudaGetLastError());
+    SCRS_CUDA(run_wht(wa, ts, D, 1, 1, d_known, log_walsh, ex, values, derivs, st));
+    SCRS_CUDA(run_wht(wa, ts, D, 0, 2, d_known, log_walsh, ex, values, derivs, st));
     return SCRS_OK;
 }
 
@@ -836,17 +940,19 @@ int32_t AfftCodec::init(uint64_t k_, uint64_t m_, uint64_t L_, scrs_error* err) 
     if (log_ts) fill_factors(f, polys, 1, (int)log_ts, 0);
     SCRS_CUDA(factors.ensure(ts * 2));
     SCRS_CUDA(cudaMemcpy(factors.p, f.data(), ts * 2, cudaMemcpyHostToDevice));
+    const std::vector<uint32_t> lw = log_walsh_host((uint32_t)ts, (int)log_ts);
+    SCRS_CUDA(log_walsh.ensure(ts * 4));
+    SCRS_CUDA(cudaMemcpy(log_walsh.p, lw.data(), ts * 4, cudaMemcpyHostToDevice));
     // Encode locator: known = [0, k), erased = [k, ts), fixed per geometry.
     SCRS_CUDA(enc_values.ensure(ts * 2));
     SCRS_CUDA(enc_derivs.ensure(ts * 2));
-    DevBuf known, wa, wb;
+    DevBuf known, wa;
     std::vector<uint8_t> hk(ts, 0);
     std::fill(hk.begin(), hk.begin() + k, 1);
     SCRS_CUDA(known.ensure(ts));
     SCRS_CUDA(wa.ensure(ts * 4));
-    SCRS_CUDA(wb.ensure(ts * 4));
     SCRS_CUDA(cudaMemcpy(known.p, hk.data(), ts, cudaMemcpyHostToDevice));
-    int32_t r = afft_locator_device(known.as<uint8_t>(), (uint32_t)ts, wa.as<uint32_t>(), wb.as<uint32_t>(),
+    int32_t r = afft_locator_device(known.as<uint8_t>(), (uint32_t)ts, log_walsh.as<uint32_t>(), wa.as<uint32_t>(),
                                     enc_values.as<uint16_t>(), enc_derivs.as<uint16_t>(), 0, err);
     if (r) return r;
     // Systematic locator for the targeted decode: known = [k, ts), erased = [0, k).
@@ -855,7 +961,7 @@ int32_t AfftCodec::init(uint64_t k_, uint64_t m_, uint64_t L_, scrs_error* err) 
     SCRS_CUDA(cudaStreamSynchronize(0));  // `known` is rewritten below
     for (uint64_t i = 0; i < ts; i++) hk[i] = i >= k ? 1 : 0;
     SCRS_CUDA(cudaMemcpy(known.p, hk.data(), ts, cudaMemcpyHostToDevice));
-    r = afft_locator_device(known.as<uint8_t>(), (uint32_t)ts, wa.as<uint32_t>(), wb.as<uint32_t>(),
+    r = afft_locator_device(known.as<uint8_t>(), (uint32_t)ts, log_walsh.as<uint32_t>(), wa.as<uint32_t>(),
                             sys_values.as<uint16_t>(), sys_derivs.as<uint16_t>(), 0, err);
     if (r) return r;
     SCRS_CUDA(cudaStreamSynchronize(0));  // the locators ran on the legacy stream
@@ -906,7 +1012,6 @@ int32_t AfftWorkspace::init_decode(const AfftCodec& c, scrs_error* err) {
     SCRS_CUDA(work1.ensure(c.ts * G * 64));
     SCRS_CUDA(known.ensure(c.ts));
     SCRS_CUDA(wht_a.ensure(c.ts * 4));
-    SCRS_CUDA(wht_b.ensure(c.ts * 4));
     SCRS_CUDA(values.ensure(c.ts * 2));
     SCRS_CUDA(derivs.ensure(c.ts * 2));
     SCRS_CUDA(row_map.ensure(c.n * 2));
@@ -1022,8 +1127,8 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
     SCRS_CUDA(cudaMemcpyAsync(ws.known.p, known, ts, cudaMemcpyHostToDevice, st));
     rc = ws.stage_release(st, err);
     if (rc) return rc;
-    int32_t r = afft_locator_device(ws.known.as<uint8_t>(), (uint32_t)ts, ws.wht_a.as<uint32_t>(),
-                                    ws.wht_b.as<uint32_t>(), ws.values.as<uint16_t>(), ws.derivs.as<uint16_t>(), st,
+    int32_t r = afft_locator_device(ws.known.as<uint8_t>(), (uint32_t)ts, log_walsh.as<uint32_t>(),
+                                    ws.wht_a.as<uint32_t>(), ws.values.as<uint16_t>(), ws.derivs.as<uint16_t>(), st,
                                     err);
     if (r) return r;
     PassIo in{};

@@ -41,6 +41,7 @@ class AfftCodec {
     uint64_t k = 0, m = 0, n = 0, L = 0, padded_k = 0, ts = 0;
     uint32_t log_ts = 0;
     DevBuf factors;                 // uint16[ts], heap layout (transform.rs:30-61)
+    DevBuf log_walsh;               // uint32[ts]: transformed log table, times 1/ts (decoder.rs:691-703)
     uint16_t deriv_factors[16] = {};
     DevBuf enc_values, enc_derivs;  // encode locator for E = [k, ts): uint16[ts]
     // Systematic locator L_S(x) = prod_{i<k}(x + i) (decoder.rs:256-266):
@@ -70,7 +71,7 @@ class AfftWorkspace {
     size_t off_map = 0, off_known = 0, off_lists = 0;  // byte offsets in an area (rows at 0)
     DevBuf work0, work1;            // ts * L bytes, bit-sliced rows
     DevBuf known;                   // uint8[ts]
-    DevBuf wht_a, wht_b;            // uint32[ts]
+    DevBuf wht_a;                   // uint32[ts]: locator transform (ts > 16384)
     DevBuf values, derivs;          // uint16[ts]
     DevBuf rows;                    // uint16 lists for the output stage
     DevBuf row_map;                 // uint16[n] codeword index -> payload row
@@ -80,7 +81,9 @@ class AfftWorkspace {
 
 // Locator evaluations for a known-point mask (decoder.rs:672-714), on the
 // device: values[x] = L(x) for known x, derivs[x] = L'(x) for erased x.
-int32_t afft_locator_device(const uint8_t* d_known, uint32_t ts, uint32_t* wa, uint32_t* wb, uint16_t* values,
-                            uint16_t* derivs, cudaStream_t st, scrs_error* err);
+// log_walsh: the codec's transformed log table; wa: uint32[ts] of work space
+// (used when ts > 16384).
+int32_t afft_locator_device(const uint8_t* d_known, uint32_t ts, const uint32_t* log_walsh, uint32_t* wa,
+                            uint16_t* values, uint16_t* derivs, cudaStream_t st, scrs_error* err);
 
 }  // namespace scrs
