@@ -116,6 +116,14 @@ __device__ __forceinline__ uint32_t add_mod(uint32_t a, uint32_t b) {
 }
 __device__ __forceinline__ uint32_t sub_mod(uint32_t a, uint32_t b) { return a >= b ? a - b : a + kMult - b; }
 
+// Programmatic dependent launch: a kernel launched with the programmatic
+// stream serialization attribute may start while the kernel before it on the
+// stream is still running.  It reads nothing that kernel writes before
+// pdl_wait(), which returns once that kernel has completed and its writes are
+// visible; pdl_trigger() lets the next such kernel start its own prologue.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // ---- erasure locator (decoder.rs:672-755) ----------------------------------------
 // log L(x) for every point x is a Walsh-Hadamard transform (mod 65535) of the
 // product of two transforms: one of the erasure indicator, one of the
@@ -346,6 +354,8 @@ struct DerivFactors {
 
 __global__ void __launch_bounds__(128) derivative_kernel(const uint8_t* in, uint8_t* out, uint32_t ts, uint32_t G,
                                                          int D, DerivFactors df) {
+    pdl_trigger();
+    pdl_wait();  // `in` is the transform pass's output
     const uint64_t total = (uint64_t)ts * G;
     for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < total;
          x += (uint64_t)gridDim.x * blockDim.x) {
@@ -485,6 +495,22 @@ __global__ void __launch_bounds__(kTileThreads) afft_tile_kernel(uint8_t* work, 
     // iterations (x0 is the warp's first element), lanes past the end with
     // nothing to do, so that mul16_lanes always has all 32 lanes.
     const uint32_t lane = tid & 31u;
+    // The node factors of the pass, after the tile: at tile level lam the rows
+    // whose level bits above the pair bit read u share factor
+    // factors[(root << l) + (hi << lam) + u]; entry (1 << lam) - 1 + u of the
+    // phase's table, 2^c - 1 entries per phase.
+    uint16_t* fac = reinterpret_cast<uint16_t*>(tile + (size_t)rows * gt * 64);
+    const uint32_t per_phase = (1u << c) - 1u;
+    for (uint32_t x = tid; x < (uint32_t)ph.n * per_phase; x += blockDim.x) {
+        const uint32_t p = x / per_phase, at = x - p * per_phase;
+        const int lam = 31 - __clz(at + 1);
+        const uint32_t u = at + 1 - (1u << lam);
+        fac[x] = factors[((uint64_t)ph.root[p] << (l0 + lam)) + ((uint64_t)hi << lam) + u];
+    }
+    // the node factors are fixed per transform; the rows are the previous
+    // kernel's output
+    pdl_trigger();
+    pdl_wait();
     if (slice) {
         for (uint32_t x0 = tid - lane; x0 < rows * gn; x0 += blockDim.x) {
             const uint32_t x = x0 + lane;
@@ -516,18 +542,6 @@ __global__ void __launch_bounds__(kTileThreads) afft_tile_kernel(uint8_t* work, 
             const uint32_t q = x & 3, g = (x >> 2) % gn, i = (x >> 2) / gn;
             cp_async_16(piece(i, q, g), work + ((uint64_t)row_of(i) * G + g0 + g) * 64 + 16 * q);
         }
-    }
-    // The node factors of the pass, after the tile: at tile level lam the rows
-    // whose level bits above the pair bit read u share factor
-    // factors[(root << l) + (hi << lam) + u]; entry (1 << lam) - 1 + u of the
-    // phase's table, 2^c - 1 entries per phase.
-    uint16_t* fac = reinterpret_cast<uint16_t*>(tile + (size_t)rows * gt * 64);
-    const uint32_t per_phase = (1u << c) - 1u;
-    for (uint32_t x = tid; x < (uint32_t)ph.n * per_phase; x += blockDim.x) {
-        const uint32_t p = x / per_phase, at = x - p * per_phase;
-        const int lam = 31 - __clz(at + 1);
-        const uint32_t u = at + 1 - (1u << lam);
-        fac[x] = factors[((uint64_t)ph.root[p] << (l0 + lam)) + ((uint64_t)hi << lam) + u];
     }
     if (!slice) cp_async_wait_all();
     __syncthreads();
@@ -622,6 +636,22 @@ int grid_for(uint64_t items, int threads) {
     return (int)std::max<uint64_t>(1, std::min<uint64_t>(g, 148ull * 32));
 }
 
+cudaError_t launch_derivative(const uint8_t* in, uint8_t* out, uint32_t ts, uint32_t G, int D,
+                              const uint16_t* deriv_factors, cudaStream_t st) {
+    DerivFactors df{};
+    std::copy(deriv_factors, deriv_factors + 16, df.f);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid_for((uint64_t)ts * G, 128));
+    cfg.blockDim = dim3(128);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, derivative_kernel, in, out, ts, G, D, df);
+}
+
 int log2_floor(uint32_t v) {
     int r = 0;
     while (v >>= 1) r++;
@@ -684,8 +714,17 @@ cudaError_t launch_pass(uint8_t* work, uint32_t G, int D, const PassPlan& P, uin
     // one butterfly per thread and level: a multiple of 32 threads, at most kTileThreads
     const uint32_t bfly = (uint32_t)(rows / 2) * gt;
     const int threads = (int)std::min<uint32_t>(kTileThreads, std::max<uint32_t>(32, (bfly + 31) / 32 * 32));
-    afft_tile_kernel<<<tiles, threads, smem, st>>>(work, G, D, P.l0, P.c, P.e, gt, ph, factors, io, slice, unslice);
-    return cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(tiles);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, afft_tile_kernel, work, G, D, P.l0, P.c, P.e, gt, ph, factors, io, slice, unslice);
 }
 
 // Full transform of 2^D bit-sliced rows (heap root `root`: 1 for the whole
@@ -1059,11 +1098,8 @@ int32_t AfftCodec::encode(const uint8_t* d_data, uint8_t* d_repairs, AfftWorkspa
     in.n_src = (uint32_t)k;
     in.L = L;
     SCRS_CUDA(run_transform(ws.work0.as<uint8_t>(), G, (int)log_ts, factors.as<uint16_t>(), false, st, 1, in));
-    DerivFactors df{};
-    std::copy(deriv_factors, deriv_factors + 16, df.f);
-    derivative_kernel<<<grid_for(ts * G, 128), 128, 0, st>>>(ws.work0.as<uint8_t>(), ws.work1.as<uint8_t>(),
-                                                             (uint32_t)ts, G, (int)log_ts, df);
-    SCRS_CUDA(cudaGetLastError());
+    SCRS_CUDA(launch_derivative(ws.work0.as<uint8_t>(), ws.work1.as<uint8_t>(), (uint32_t)ts, G, (int)log_ts,
+                                deriv_factors, st));
     PassIo out{};
     out.known = ws.known.as<uint8_t>();
     out.out_lo = (uint32_t)k;
@@ -1139,11 +1175,8 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
     in.n_src = (uint32_t)ts;
     in.L = L;
     SCRS_CUDA(run_transform(ws.work0.as<uint8_t>(), G, (int)log_ts, factors.as<uint16_t>(), false, st, 1, in));
-    DerivFactors df{};
-    std::copy(deriv_factors, deriv_factors + 16, df.f);
-    derivative_kernel<<<grid_for(ts * G, 128), 128, 0, st>>>(ws.work0.as<uint8_t>(), ws.work1.as<uint8_t>(),
-                                                             (uint32_t)ts, G, (int)log_ts, df);
-    SCRS_CUDA(cudaGetLastError());
+    SCRS_CUDA(launch_derivative(ws.work0.as<uint8_t>(), ws.work1.as<uint8_t>(), (uint32_t)ts, G, (int)log_ts,
+                                deriv_factors, st));
     // the missing data rows: rows of [0, k) not known
     PassIo out{};
     out.known = ws.known.as<uint8_t>();
