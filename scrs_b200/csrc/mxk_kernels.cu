@@ -67,10 +67,17 @@ __device__ __forceinline__ void load_out_planes(const uint8_t* orow, uint64_t of
 // second pass over the staged rows.  The warp runs a step list of
 // (i * chunk bytes) | (u-flag << 4) | nibble entries: the high-nibble pass,
 // the x16 fold, then the low-nibble pass.
+//
+// Between the segments of a stripe whose chunk is a whole aligned span of the
+// row (`sliced_in` / `sliced_out`), the partial sum stays in the output row
+// in bit-sliced form: each lane stores its plane words where its bytes go and
+// reads them back for the next segment, so only the last segment converts
+// back to bytes.
 template <int kGf16>
 __device__ __forceinline__ void output_row(const uint8_t* buf, uint32_t c, uint16_t* steps, uint32_t seg_n, int lane,
                                            bool existing, uint8_t* orow, uint64_t off, uint64_t L, bool aligned,
-                                           bool full, bool atomic_out) {
+                                           bool full, bool atomic_out, bool sliced_in = false,
+                                           bool sliced_out = false) {
     using G = FieldGeom<kGf16>;
     using Words = typename Lane<kGf16>::Words;
     constexpr int kWords = Lane<kGf16>::kWords;
@@ -128,13 +135,25 @@ __device__ __forceinline__ void output_row(const uint8_t* buf, uint32_t c, uint1
             }
             if (existing) {
                 Words e;
-                load_out_planes<kGf16>(orow, off, lane, L, aligned, e);
+                if (sliced_in) {
+#pragma unroll
+                    for (int pc = 0; pc < Lane<kGf16>::kPieces; pc++) {
+                        const uint4 v = *reinterpret_cast<const uint4*>(orow + off + piece_pos(pc, lane));
+                        e[4 * pc] = v.x, e[4 * pc + 1] = v.y, e[4 * pc + 2] = v.z, e[4 * pc + 3] = v.w;
+                    }
+                } else {
+                    load_out_planes<kGf16>(orow, off, lane, L, aligned, e);
+                }
 #pragma unroll
                 for (int t = 0; t < kWords; t++) acc[t] ^= e[t];
             }
         }
     }
     __syncwarp();  // the list is rebuilt for the warp's next output row
+    if (sliced_out) {
+        store_pieces<Lane<kGf16>::kPieces>(orow, off, 0, lane, L, true, true, acc);
+        return;
+    }
     bitslice_lane<kGf16>(acc);
     if (atomic_out) {  // partial sum of an input range: XOR into the (zeroed) output
 #pragma unroll
@@ -230,12 +249,18 @@ __device__ bool process_item(const MxkTask& T, uint32_t chunk, uint8_t* buf, uin
             }
             __syncthreads();
             // ---- output rows, one per warp at a time
+            // partial sums between segments stay bit-sliced when the chunk is
+            // a whole aligned span of the row
+            const bool sliced = !(kShape & kShapeOneSeg) && !atomic_out && full;
+            const bool sliced_in = sliced && seg != in_lo;
+            const bool sliced_out = sliced && seg + (uint32_t)seg_cap < n_in;
             for (uint32_t j = warp; j < og_n; j += 4) {
                 if (j != (uint32_t)warp) c = lane_coef<kGf16>(T, seg, seg_n, og, j, lane);
                 const uint32_t orow_idx = T.out_rows ? T.out_rows[og + j] : og + j;
                 output_row<kGf16>(buf, c, steps, seg_n, lane,
                                   !(kShape & kShapeOneSeg) && !atomic_out && (seg != in_lo || T.accumulate),
-                                  T.out + (uint64_t)orow_idx * T.out_stride, off, L, aligned, full, atomic_out);
+                                  T.out + (uint64_t)orow_idx * T.out_stride, off, L, aligned, full, atomic_out,
+                                  sliced_in, sliced_out);
             }
             __syncthreads();
         }
