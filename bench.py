@@ -47,6 +47,8 @@ METRIC = "encode/decode GB/s and HBM-roofline % on 1 B200; batched vs plain; p50
 K, M, L = 10, 4, 4096
 STRIPES = 65536
 MIXED_STRIPES = 8192  # stripes of the mixed batch; smaller values are for ncu captures
+ENVELOPE_CELLS = None  # (k, m) cells of the GF(256) envelope; None: the full 3 x 3 sweep
+ENVELOPE_BYTES = 512 << 20  # input bytes per envelope cell
 SEED = 0x5C250001
 
 
@@ -1026,7 +1028,7 @@ def extra_afft(torch, api, cpu=None):
     return res
 
 
-def extra_sweep(torch, api, cpu=None, ks=(10, 32, 64), ms=(4, 8, 16), Ls=4096, in_bytes=512 << 20):
+def extra_sweep(torch, api, cpu=None, ks=(10, 32, 64), ms=(4, 8, 16), Ls=4096, in_bytes=None):
     """The GF(256) envelope: for each (k, m), a batch of Good Cauchy stripes
     (L = 4 KiB, enough stripes for about 512 MB of input, far above L2) run
     as encodes and, separately, as batch decodes from seeded random k-of-n
@@ -1039,48 +1041,49 @@ def extra_sweep(torch, api, cpu=None, ks=(10, 32, 64), ms=(4, 8, 16), Ls=4096, i
 
     peak = peaks()[0]
     eng = int(Engine.GOOD_CAUCHY)
+    in_bytes = ENVELOPE_BYTES if in_bytes is None else in_bytes
+    grid = ENVELOPE_CELLS or [(k, m) for k in ks for m in ms]
     cells, ok = [], True
-    for k in ks:
-        for m in ms:
-            n = max(1, in_bytes // (k * Ls))
-            gen = torch.Generator(device="cuda")
-            gen.manual_seed(SEED + 100 + k * 17 + m)
-            data = torch.randint(0, 256, (n, k * Ls), dtype=torch.uint8, device="cuda", generator=gen)
-            reps = torch.zeros((n, m * Ls), dtype=torch.uint8, device="cuda")
-            idx = np.arange(n, dtype=np.uint64)
-            b = StripeBatch(api.lib, n)
-            b.set_arrays(np.full(n, OP_ENCODE), np.full(n, eng), np.full(n, k), np.full(n, m), np.full(n, Ls),
-                         data.data_ptr() + idx * (k * Ls), reps.data_ptr() + idx * (m * Ls))
-            b.run()
-            torch.cuda.synchronize()
-            enc = [b.run_timed_drains() for _ in range(5)]
-            t_enc = float(np.median([r[1] + r[2] for r in enc]))
-            spec = b.jit_stripes > 0
-            rng = np.random.default_rng(SEED + 200 + k * 17 + m)
-            recv = np.argsort(rng.random((n, k + m)), axis=1)[:, :k].astype(np.int64)
-            word = torch.cat([data.view(n, k, Ls), reps.view(n, m, Ls)], dim=1)
-            received = word[torch.arange(n, device="cuda")[:, None], torch.from_numpy(recv).cuda()].reshape(n, k * Ls)
-            del word
-            out = torch.zeros((n, k * Ls), dtype=torch.uint8, device="cuda")
-            b.set_arrays(np.full(n, OP_DECODE), np.full(n, eng), np.full(n, k), np.full(n, m), np.full(n, Ls),
-                         received.data_ptr() + idx * (k * Ls), out.data_ptr() + idx * (k * Ls),
-                         indices=recv.astype(np.uint16))
-            b.run()
-            torch.cuda.synchronize()
-            ok &= bool(torch.equal(out, data))
-            dec = [b.run_timed_drains() for _ in range(5)]
-            t_dec = float(np.median([r[2] for r in dec]))
-            plan = float(np.median([r[0] for r in dec]))
-            b.check()
-            enc_bytes, dec_bytes = n * (k + m) * Ls, n * 2 * k * Ls
-            cells.append({"k": k, "m": m, "stripes": n,
-                          "encode_ms": round(t_enc, 4), "encode_frac": round(enc_bytes / t_enc / 1e6 / peak, 3),
-                          "encode_kernel": "scrs_spec_drain" if spec else "mxk_kernel<0>",
-                          "decode_ms": round(t_dec, 4), "decode_frac": round(dec_bytes / t_dec / 1e6 / peak, 3),
-                          "decode_plan_ms": round(plan, 4),
-                          "mean_erased": round(float((recv >= k).sum()) / n, 2)})
-            del data, reps, received, out, b
-            torch.cuda.empty_cache()
+    for k, m in grid:
+        n = max(1, in_bytes // (k * Ls))
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(SEED + 100 + k * 17 + m)
+        data = torch.randint(0, 256, (n, k * Ls), dtype=torch.uint8, device="cuda", generator=gen)
+        reps = torch.zeros((n, m * Ls), dtype=torch.uint8, device="cuda")
+        idx = np.arange(n, dtype=np.uint64)
+        b = StripeBatch(api.lib, n)
+        b.set_arrays(np.full(n, OP_ENCODE), np.full(n, eng), np.full(n, k), np.full(n, m), np.full(n, Ls),
+                     data.data_ptr() + idx * (k * Ls), reps.data_ptr() + idx * (m * Ls))
+        b.run()
+        torch.cuda.synchronize()
+        enc = [b.run_timed_drains() for _ in range(5)]
+        t_enc = float(np.median([r[1] + r[2] for r in enc]))
+        spec = b.jit_stripes > 0
+        rng = np.random.default_rng(SEED + 200 + k * 17 + m)
+        recv = np.argsort(rng.random((n, k + m)), axis=1)[:, :k].astype(np.int64)
+        word = torch.cat([data.view(n, k, Ls), reps.view(n, m, Ls)], dim=1)
+        received = word[torch.arange(n, device="cuda")[:, None], torch.from_numpy(recv).cuda()].reshape(n, k * Ls)
+        del word
+        out = torch.zeros((n, k * Ls), dtype=torch.uint8, device="cuda")
+        b.set_arrays(np.full(n, OP_DECODE), np.full(n, eng), np.full(n, k), np.full(n, m), np.full(n, Ls),
+                     received.data_ptr() + idx * (k * Ls), out.data_ptr() + idx * (k * Ls),
+                     indices=recv.astype(np.uint16))
+        b.run()
+        torch.cuda.synchronize()
+        ok &= bool(torch.equal(out, data))
+        dec = [b.run_timed_drains() for _ in range(5)]
+        t_dec = float(np.median([r[2] for r in dec]))
+        plan = float(np.median([r[0] for r in dec]))
+        b.check()
+        enc_bytes, dec_bytes = n * (k + m) * Ls, n * 2 * k * Ls
+        cells.append({"k": k, "m": m, "stripes": n,
+                      "encode_ms": round(t_enc, 4), "encode_frac": round(enc_bytes / t_enc / 1e6 / peak, 3),
+                      "encode_kernel": "scrs_spec_drain" if spec else "mxk_kernel<0>",
+                      "decode_ms": round(t_dec, 4), "decode_frac": round(dec_bytes / t_dec / 1e6 / peak, 3),
+                      "decode_plan_ms": round(plan, 4),
+                      "mean_erased": round(float((recv >= k).sum()) / n, 2)})
+        del data, reps, received, out, b
+        torch.cuda.empty_cache()
     return {"workload": "Good Cauchy stripes, L=4096, ~512 MB of input per cell; encode and batch decode (seeded "
                         "random k-of-n receipt sets) as persistent launches; drain time by CUDA events",
             "peak_GBps": peak, "cells": cells, "bit_exact": ok}
@@ -1204,7 +1207,7 @@ def run_ours(args, world, rank, local):
                                       "stripe), so e2e cannot exceed the host-to-device copy rate measured alone "
                                       "(1 GiB pinned copy, CUDA events)"},
                "path": "scrs_stripe_batch_set_host + scrs_stripe_batch_run (pinned host buffers; copies of "
-                       "32 pieces overlap the compute, both copy directions at once; decode stripes copy back "
+                       "64 pieces overlap the compute, both copy directions at once; decode stripes copy back "
                        "only their missing rows, their present rows are copied host-side while the GPU runs)"}
         launches += hb.last_launches * n_e2e
     extras = {}
@@ -1263,7 +1266,7 @@ def run_reference(args, world, rank):
 
 
 def main():
-    global STRIPES, MIXED_STRIPES
+    global STRIPES, MIXED_STRIPES, ENVELOPE_CELLS, ENVELOPE_BYTES
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
@@ -1277,11 +1280,18 @@ def main():
     ap.add_argument("--mixed-stripes", type=int, default=MIXED_STRIPES,
                     help="stripes of the mixed batch extra; the reported figure uses 8192, smaller values are for ncu "
                          "captures")
+    ap.add_argument("--envelope-cells", default=None,
+                    help="GF(256) envelope cells as KxM[,KxM...] (default: the full sweep); for ncu captures")
+    ap.add_argument("--envelope-mb", type=int, default=ENVELOPE_BYTES >> 20,
+                    help="input MB per envelope cell (default 512; keep above the 126 MB L2)")
     ap.add_argument("--only", choices=sorted(EXTRAS),
                     help="run just one of the extras and print its JSON (profiling runs; no headline line)")
     args = ap.parse_args()
     STRIPES = args.stripes
     MIXED_STRIPES = args.mixed_stripes
+    if args.envelope_cells:
+        ENVELOPE_CELLS = [tuple(int(v) for v in c.split("x")) for c in args.envelope_cells.split(",")]
+    ENVELOPE_BYTES = args.envelope_mb << 20
     if args.only:
         import torch
         import scrs_b200

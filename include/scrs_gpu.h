@@ -391,7 +391,7 @@ SCRS_API int32_t scrs_stripe_batch_set(scrs_stripe_batch* batch,
 /* Host-buffer form of scrs_stripe_batch_set: every `in` / `out` pointer is
  * HOST memory (pinned memory gives asynchronous copies).  The batch owns
  * device staging sized at this call.  Each run cuts the stripes into up to
- * 32 pieces of about equal input bytes and pipelines them: the inputs of
+ * 64 pieces of about equal input bytes and pipelines them: the inputs of
  * piece p+1 are copied in and the outputs of piece p-1 copied out (on two
  * internal streams) while piece p computes; the run's stream waits for the
  * last copy.  Copies of stripes that are contiguous in host memory are

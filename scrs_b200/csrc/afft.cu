@@ -450,19 +450,24 @@ struct PassIo {
 // is valid there: all active lanes share the index); with more, every lane
 // runs the branch-free product (mul16_masked), whose cost does not grow with
 // the number of factors.
-__device__ __forceinline__ void mul16_lanes(uint32_t f, uint32_t (&acc)[16], const uint32_t (&x)[16]) {
+// `uniform`: the caller knows every lane holds the same f (block-uniform
+// flag), so the warp skips the match and ballots on its critical path.
+__device__ __forceinline__ void mul16_lanes(uint32_t f, uint32_t (&acc)[16], const uint32_t (&x)[16],
+                                            bool uniform = false) {
     const int lane = threadIdx.x & 31;
-    const unsigned same = __match_any_sync(0xFFFFFFFFu, f);
-    const unsigned leaders = __ballot_sync(0xFFFFFFFFu, (unsigned)(__ffs(same) - 1) == (unsigned)lane);
-    if (__popc(leaders) > 2) {
-        if (f) mul16_masked(f, acc, x);
-        return;
+    if (!uniform) {
+        const unsigned same = __match_any_sync(0xFFFFFFFFu, f);
+        const unsigned leaders = __ballot_sync(0xFFFFFFFFu, (unsigned)(__ffs(same) - 1) == (unsigned)lane);
+        if (__popc(leaders) > 2) {
+            if (f) mul16_masked(f, acc, x);
+            return;
+        }
     }
     unsigned left = 0xFFFFFFFFu;
     while (left) {
-        const uint32_t fl = __shfl_sync(0xFFFFFFFFu, f, __ffs(left) - 1);
-        const bool mine = ((left >> lane) & 1u) && f == fl;
-        const unsigned grp = __ballot_sync(0xFFFFFFFFu, mine);
+        const uint32_t fl = uniform ? f : __shfl_sync(0xFFFFFFFFu, f, __ffs(left) - 1);
+        const bool mine = uniform || (((left >> lane) & 1u) && f == fl);
+        const unsigned grp = uniform ? 0xFFFFFFFFu : __ballot_sync(0xFFFFFFFFu, mine);
         if (mine && fl) mul16<true>(fl, acc, x);
         left &= ~grp;
     }
@@ -554,6 +559,10 @@ __global__ void __launch_bounds__(kTileThreads) afft_tile_kernel(uint8_t* work, 
             const int lam = fwd ? s : c - 1 - s;  // tile-local level
             const int b = c - 1 - lam;            // pair bit among the level bits
             const uint16_t* lf = fac + p * per_phase + (1u << lam) - 1u;
+            // every warp holds one factor when its 32 items agree in all bits
+            // from the pair bit up: items (low bits, group) of 2^(e+b) * gn
+            // share the factor index r >> b
+            const bool uni = gpow && (items & 31u) == 0 && ((gn << e) << b) >= 32u;
             for (uint32_t x0 = tid - lane; x0 < items; x0 += blockDim.x) {
                 const uint32_t x = x0 + lane;
                 const bool valid = x < items;
@@ -577,7 +586,7 @@ __global__ void __launch_bounds__(kTileThreads) afft_tile_kernel(uint8_t* work, 
 #pragma unroll
                     for (int q = 0; q < 16; q++) wh[q] ^= wl[q];
                 }
-                mul16_lanes(f, wl, wh);
+                mul16_lanes(f, wl, wh, uni);
                 if (fwd) {
 #pragma unroll
                     for (int q = 0; q < 16; q++) wh[q] ^= wl[q];
@@ -1016,10 +1025,6 @@ int32_t AfftWorkspace::init_encode(const AfftCodec& c, scrs_error* err) {
     std::vector<uint8_t> hk(c.ts, 0);
     std::fill(hk.begin(), hk.begin() + c.k, 1);
     SCRS_CUDA(upload_now(known.p, hk.data(), c.ts));
-    std::vector<uint16_t> host_rows(2 * c.m);
-    for (uint64_t t = 0; t < c.m; t++) host_rows[t] = (uint16_t)(c.k + t), host_rows[c.m + t] = (uint16_t)t;
-    SCRS_CUDA(rows.ensure(host_rows.size() * 2));
-    SCRS_CUDA(upload_now(rows.p, host_rows.data(), host_rows.size() * 2));
     return SCRS_OK;
 }
 
@@ -1049,13 +1054,11 @@ int32_t AfftWorkspace::init_decode(const AfftCodec& c, scrs_error* err) {
     const uint64_t G = (c.L + 63) / 64;
     SCRS_CUDA(work0.ensure(c.ts * G * 64));
     SCRS_CUDA(work1.ensure(c.ts * G * 64));
-    SCRS_CUDA(known.ensure(c.ts));
     SCRS_CUDA(wht_a.ensure(c.ts * 4));
     SCRS_CUDA(values.ensure(c.ts * 2));
     SCRS_CUDA(derivs.ensure(c.ts * 2));
-    SCRS_CUDA(row_map.ensure(c.n * 2));
     const size_t rows_bytes = (2 * c.k + 8) * 2;
-    const size_t lists_elems = 3 * c.k + 4 * kTargetedMax + kTargetedMax * kTargetedMax + 8;
+    const size_t lists_elems = c.targeted_list_elems();
     off_map = (rows_bytes + 15) & ~(size_t)15;
     off_known = (off_map + c.n * 2 + 15) & ~(size_t)15;
     off_lists = (off_known + c.ts + 15) & ~(size_t)15;
@@ -1064,10 +1067,9 @@ int32_t AfftWorkspace::init_decode(const AfftCodec& c, scrs_error* err) {
         memset(stage[i].p, 0, stage[i].bytes);
         if (!staged[i]) SCRS_CUDA(cudaEventCreateWithFlags(&staged[i], cudaEventDisableTiming));
     }
-    SCRS_CUDA(rows.ensure(rows_bytes));
+    SCRS_CUDA(up.ensure(off_lists + lists_elems * 2));
     SCRS_CUDA(tgen.ensure(kTargetedMax * c.k * 2));
     SCRS_CUDA(tcoef.ensure(kTargetedMax * c.k * 2));
-    SCRS_CUDA(tlists.ensure((3 * c.k + 4 * kTargetedMax + kTargetedMax * kTargetedMax + 8) * 2));
     return SCRS_OK;
 }
 
@@ -1132,14 +1134,35 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
         else
             miss[nm++] = (uint16_t)d;
     }
-    SCRS_CUDA(cudaMemcpyAsync(ws.rows.p, miss, (2 * k + 8) * 2, cudaMemcpyHostToDevice, st));
-    const uint16_t* d_pres = ws.rows.as<uint16_t>() + k;
-    const uint16_t* d_map = nullptr;
+    // Everything the decode uploads sits in one stage area laid out as its
+    // device mirror (rows | codeword -> payload map | known mask | targeted
+    // lists), so it goes up in one copy.
+    size_t upload = (2 * k + 8) * 2;
     if (row_map) {
         memcpy(stage + ws.off_map, row_map, n * 2);
-        SCRS_CUDA(cudaMemcpyAsync(ws.row_map.p, stage + ws.off_map, n * 2, cudaMemcpyHostToDevice, st));
-        d_map = ws.row_map.as<uint16_t>();
+        upload = ws.off_map + n * 2;
     }
+    const bool targeted = nm > 0 && nm <= kTargetedMax;
+    if (targeted) {
+        rc = targeted_lists(have, ws, err, row_map, miss, nm, pres, np);
+        if (rc) {
+            const int32_t rr = ws.stage_release(st, err);
+            return rc ? rc : rr;
+        }
+        upload = ws.off_lists + targeted_list_elems() * 2;
+    } else if (nm > 0) {
+        uint8_t* known = stage + ws.off_known;
+        memcpy(known, have, n);  // receipt flags are 0 / 1
+        memset(known + n, 0, ts - n);
+        upload = ws.off_known + ts;
+    }
+    SCRS_CUDA(cudaMemcpyAsync(ws.up.p, stage, upload, cudaMemcpyHostToDevice, st));
+    rc = ws.stage_release(st, err);
+    if (rc) return rc;
+    const uint8_t* dev = ws.up.as<uint8_t>();
+    const uint16_t* d_pres = reinterpret_cast<const uint16_t*>(dev) + k;
+    const uint16_t* d_map = row_map ? reinterpret_cast<const uint16_t*>(dev + ws.off_map) : nullptr;
+    const uint8_t* d_known = dev + ws.off_known;
     if (np) {
         const bool vec = L % 16 == 0 && (reinterpret_cast<uintptr_t>(d_payloads) & 15) == 0 &&
                          (reinterpret_cast<uintptr_t>(d_out) & 15) == 0;
@@ -1151,25 +1174,14 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
                                                                                    d_map);
         SCRS_CUDA(cudaGetLastError());
     }
-    if (nm == 0) return ws.stage_release(st, err);
-    if (nm <= kTargetedMax) {
-        rc = decode_targeted(d_payloads, have, d_out, ws, status, st, err, row_map, miss, nm, pres, np);
-        const int32_t rr = ws.stage_release(st, err);  // after its list upload, on every path
-        return rc ? rc : rr;
-    }
-    uint8_t* known = stage + ws.off_known;
-    memcpy(known, have, n);  // receipt flags are 0 / 1
-    memset(known + n, 0, ts - n);
-    SCRS_CUDA(cudaMemcpyAsync(ws.known.p, known, ts, cudaMemcpyHostToDevice, st));
-    rc = ws.stage_release(st, err);
-    if (rc) return rc;
-    int32_t r = afft_locator_device(ws.known.as<uint8_t>(), (uint32_t)ts, log_walsh.as<uint32_t>(),
-                                    ws.wht_a.as<uint32_t>(), ws.values.as<uint16_t>(), ws.derivs.as<uint16_t>(), st,
-                                    err);
+    if (nm == 0) return SCRS_OK;
+    if (targeted) return decode_targeted(d_payloads, d_out, ws, status, st, err, nm);
+    int32_t r = afft_locator_device(d_known, (uint32_t)ts, log_walsh.as<uint32_t>(), ws.wht_a.as<uint32_t>(),
+                                    ws.values.as<uint16_t>(), ws.derivs.as<uint16_t>(), st, err);
     if (r) return r;
     PassIo in{};
     in.src = d_payloads;
-    in.known = ws.known.as<uint8_t>();
+    in.known = d_known;
     in.row_map = d_map;
     in.in_scale = ws.values.as<uint16_t>();
     in.n_src = (uint32_t)ts;
@@ -1179,7 +1191,7 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
                                 deriv_factors, st));
     // the missing data rows: rows of [0, k) not known
     PassIo out{};
-    out.known = ws.known.as<uint8_t>();
+    out.known = d_known;
     out.out_lo = 0;
     out.out_hi = (uint32_t)k;
     out.dst = d_out;
@@ -1191,15 +1203,14 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
     return SCRS_OK;
 }
 
-int32_t AfftCodec::decode_targeted(const uint8_t* d_payloads, const uint8_t* have, uint8_t* d_out,
-                                   AfftWorkspace& ws, int32_t* status, cudaStream_t st, scrs_error* err,
-                                   const uint16_t* row_map, const uint16_t* miss, uint32_t nm, const uint16_t* pres,
-                                   uint32_t np) const {
-    const uint16_t *lg, *ex;
-    SCRS_CUDA(log16_tables(&lg, &ex));
-    // lists: in_rows[k] (repairs then present), out_rows[nm], rep[nm] (evaluation points),
-    // missing[nm], present[np]
-    const size_t n_lists = 3 * k + 4 * kTargetedMax + kTargetedMax * kTargetedMax + 8;
+// Targeted lists in the stage area (at off_lists): in_rows[k] (the received
+// repairs' payload rows, then the present data rows'), out_rows[5],
+// rep[5] (the repairs' evaluation points), missing[5], present[k], then room
+// for the r x r inverse the device writes.
+size_t AfftCodec::targeted_list_elems() const { return 3 * k + 4 * kTargetedMax + kTargetedMax * kTargetedMax + 8; }
+
+int32_t AfftCodec::targeted_lists(const uint8_t* have, AfftWorkspace& ws, scrs_error* err, const uint16_t* row_map,
+                                  const uint16_t* miss, uint32_t nm, const uint16_t* pres, uint32_t np) const {
     uint16_t* h = reinterpret_cast<uint16_t*>(ws.stage_ptr() + ws.off_lists);  // acquired by decode()
     uint16_t* in_rows = h;
     uint16_t* out_rows = in_rows + k;
@@ -1213,8 +1224,14 @@ int32_t AfftCodec::decode_targeted(const uint8_t* d_payloads, const uint8_t* hav
     auto payload_row = [&](uint32_t w) { return row_map ? row_map[w] : (uint16_t)w; };
     for (uint32_t t = 0; t < nm; t++) in_rows[t] = payload_row(rep[t]), out_rows[t] = miss[t], mis[t] = miss[t];
     for (uint32_t z = 0; z < np; z++) in_rows[nm + z] = payload_row(pres[z]), prs[z] = pres[z];
-    SCRS_CUDA(cudaMemcpyAsync(ws.tlists.p, h, n_lists * 2, cudaMemcpyHostToDevice, st));
-    const uint16_t* d_in_rows = ws.tlists.as<uint16_t>();
+    return SCRS_OK;
+}
+
+int32_t AfftCodec::decode_targeted(const uint8_t* d_payloads, uint8_t* d_out, AfftWorkspace& ws, int32_t* status,
+                                   cudaStream_t st, scrs_error* err, uint32_t nm) const {
+    const uint16_t *lg, *ex;
+    SCRS_CUDA(log16_tables(&lg, &ex));
+    const uint16_t* d_in_rows = reinterpret_cast<const uint16_t*>(ws.up.as<uint8_t>() + ws.off_lists);
     const uint16_t* d_out_rows = d_in_rows + k;
     const uint16_t* d_rep = d_out_rows + kTargetedMax;
     const uint16_t* d_mis = d_rep + kTargetedMax;

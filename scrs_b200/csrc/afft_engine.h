@@ -34,9 +34,13 @@ class AfftCodec {
                    int32_t* status, cudaStream_t st, scrs_error* err, const uint16_t* row_map = nullptr) const;
 
     // r <= 5 missing data symbols: one coefficient table + multiply-XOR pass.
-    int32_t decode_targeted(const uint8_t* d_payloads, const uint8_t* have, uint8_t* d_out, AfftWorkspace& ws,
-                            int32_t* status, cudaStream_t st, scrs_error* err, const uint16_t* row_map,
-                            const uint16_t* miss, uint32_t nm, const uint16_t* pres, uint32_t np) const;
+    // targeted_lists fills the lists in the workspace's stage area (host);
+    // decode_targeted runs the device part once they are uploaded.
+    size_t targeted_list_elems() const;
+    int32_t targeted_lists(const uint8_t* have, AfftWorkspace& ws, scrs_error* err, const uint16_t* row_map,
+                           const uint16_t* miss, uint32_t nm, const uint16_t* pres, uint32_t np) const;
+    int32_t decode_targeted(const uint8_t* d_payloads, uint8_t* d_out, AfftWorkspace& ws, int32_t* status,
+                            cudaStream_t st, scrs_error* err, uint32_t nm) const;
 
     uint64_t k = 0, m = 0, n = 0, L = 0, padded_k = 0, ts = 0;
     uint32_t log_ts = 0;
@@ -70,12 +74,11 @@ class AfftWorkspace {
     int cur = 0;
     size_t off_map = 0, off_known = 0, off_lists = 0;  // byte offsets in an area (rows at 0)
     DevBuf work0, work1;            // ts * L bytes, bit-sliced rows
-    DevBuf known;                   // uint8[ts]
+    DevBuf known;                   // uint8[ts]: the encode's known-point mask
     DevBuf wht_a;                   // uint32[ts]: locator transform (ts > 16384)
     DevBuf values, derivs;          // uint16[ts]
-    DevBuf rows;                    // uint16 lists for the output stage
-    DevBuf row_map;                 // uint16[n] codeword index -> payload row
-    DevBuf tgen, tcoef, tlists;     // targeted decode: generator rows, fused coefficients, lists
+    DevBuf up;                      // device mirror of a decode's stage area, uploaded in one copy
+    DevBuf tgen, tcoef;             // targeted decode: generator rows, fused coefficients
     uint64_t k = 0, m = 0, L = 0;
 };
 

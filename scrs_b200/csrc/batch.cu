@@ -189,7 +189,7 @@ struct scrs_stripe_batch {
 };
 
 namespace {
-constexpr size_t kMaxPieces = 32;  // one work counter each in d_counter
+constexpr size_t kMaxPieces = 64;  // one work counter each in d_counter
 constexpr size_t kMaxSpecRuns = 4;  // specialised groups per batch (counters 1..4)
 constexpr size_t kTowerCounter = 1 + kMaxSpecRuns;  // work counter of the tower drain
 

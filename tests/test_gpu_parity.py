@@ -354,7 +354,7 @@ def test_stripe_batch_with_tower_stripes(gpu, oracle):
 
 
 def test_stripe_batch_host_buffers_pipelined(gpu, oracle):
-    """Host-buffer batches run in up to 32 pieces whose copies overlap the
+    """Host-buffer batches run in up to 64 pieces whose copies overlap the
     compute; a decode stripe's present rows are copied on the host and only
     its missing rows come back from the device.  Results must equal the
     oracle's, run after run, pipelined and one launch per stripe, with decode
