@@ -49,6 +49,7 @@ STRIPES = 65536
 MIXED_STRIPES = 8192  # stripes of the mixed batch; smaller values are for ncu captures
 ENVELOPE_CELLS = None  # (k, m) cells of the GF(256) envelope; None: the full 3 x 3 sweep
 ENVELOPE_BYTES = 512 << 20  # input bytes per envelope cell
+CALL_REPS = None  # per-call extras: calls per mean / percentile (None: 20 / 200); small values for ncu launch lists
 SEED = 0x5C250001
 
 
@@ -406,6 +407,7 @@ class Cpu:
 # ---------------------------------------------------------------------------
 
 def time_ms(torch, fn, reps):
+    reps = reps if CALL_REPS is None else CALL_REPS
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     s.record()
@@ -419,6 +421,8 @@ def time_ms(torch, fn, reps):
 def per_call_ms(torch, fn, samples=200, warm=5):
     """p50 / p99 of `samples` single calls, each bracketed by CUDA events on
     the current stream and synchronised (host issue cost included)."""
+    if CALL_REPS is not None:
+        samples, warm = CALL_REPS, 0
     for _ in range(warm):
         fn()
     torch.cuda.synchronize()
@@ -1266,7 +1270,7 @@ def run_reference(args, world, rank):
 
 
 def main():
-    global STRIPES, MIXED_STRIPES, ENVELOPE_CELLS, ENVELOPE_BYTES
+    global STRIPES, MIXED_STRIPES, ENVELOPE_CELLS, ENVELOPE_BYTES, CALL_REPS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
@@ -1284,6 +1288,9 @@ def main():
                     help="GF(256) envelope cells as KxM[,KxM...] (default: the full sweep); for ncu captures")
     ap.add_argument("--envelope-mb", type=int, default=ENVELOPE_BYTES >> 20,
                     help="input MB per envelope cell (default 512; keep above the 126 MB L2)")
+    ap.add_argument("--call-reps", type=int, default=None,
+                    help="calls per mean and per percentile in the per-call extras (default 20 / 200); small "
+                         "values keep ncu launch lists short")
     ap.add_argument("--only", choices=sorted(EXTRAS),
                     help="run just one of the extras and print its JSON (profiling runs; no headline line)")
     args = ap.parse_args()
@@ -1292,6 +1299,7 @@ def main():
     if args.envelope_cells:
         ENVELOPE_CELLS = [tuple(int(v) for v in c.split("x")) for c in args.envelope_cells.split(",")]
     ENVELOPE_BYTES = args.envelope_mb << 20
+    CALL_REPS = args.call_reps
     if args.only:
         import torch
         import scrs_b200
