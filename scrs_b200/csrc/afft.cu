@@ -238,6 +238,7 @@ __global__ void __launch_bounds__(kLocatorThreads) locator_one_cta_kernel(const 
                                                                const uint16_t* exp16, uint16_t* values,
                                                                uint16_t* derivs) {
     extern __shared__ uint32_t sm_loc[];
+    pdl_trigger();  // the first transform pass may start slicing its rows
     const int r2 = D <= 5 ? 0 : min(4, D - 5);
     const int rb = D <= 9 ? 0 : D - 9;
     switch (r2 * 8 + rb) {
@@ -265,6 +266,7 @@ __global__ void __launch_bounds__(1024) wht_pass_kernel(uint32_t* v, int lo, int
                                                         const uint8_t* known, const uint32_t* lw,
                                                         const uint16_t* exp16, uint16_t* values, uint16_t* derivs) {
     extern __shared__ uint32_t sv[];
+    pdl_trigger();  // after the last pass: the first transform pass may start slicing its rows
     const uint32_t gsize = 1u << nb;
     const uint32_t gidx = blockIdx.x;
     const uint32_t base = ((gidx >> lo) << (lo + nb)) | (gidx & ((1u << lo) - 1u));
@@ -441,6 +443,11 @@ struct PassIo {
     const uint16_t* log16;
     const uint16_t* exp16;
     uint64_t L;
+    // the slice's byte rows, row map and known mask were complete before the
+    // previous kernel on the stream started (the decode's locator, itself
+    // launched without programmatic serialisation): the first pass reads them
+    // before waiting on that kernel, and waits only for in_scale
+    int32_t early_read;
 };
 
 // acc ^= f * x for every lane of the calling warp (all 32 lanes call it
@@ -513,35 +520,55 @@ __global__ void __launch_bounds__(kTileThreads) afft_tile_kernel(uint8_t* work, 
         fac[x] = factors[((uint64_t)ph.root[p] << (l0 + lam)) + ((uint64_t)hi << lam) + u];
     }
     // the node factors are fixed per transform; the rows are the previous
-    // kernel's output
+    // kernel's output, or (io.early_read) were complete before it started
     pdl_trigger();
-    pdl_wait();
     if (slice) {
-        for (uint32_t x0 = tid - lane; x0 < rows * gn; x0 += blockDim.x) {
-            const uint32_t x = x0 + lane;
-            const bool valid = x < rows * gn;
-            const uint32_t g = valid ? x % gn : 0u, i = valid ? x / gn : 0u;
+        if (!io.early_read) pdl_wait();
+        // bytes in, bit-sliced, unscaled
+        for (uint32_t x = tid; x < rows * gn; x += blockDim.x) {
+            const uint32_t g = x % gn, i = x / gn;
             const uint32_t r = row_of(i);
-            const bool have = valid && r < io.n_src && (!io.known || io.known[r]);
-            uint32_t w[16], acc[16];
+            uint32_t w[16];
 #pragma unroll
-            for (int q = 0; q < 16; q++) acc[q] = 0, w[q] = 0;
-            if (have) {
+            for (int q = 0; q < 16; q++) w[q] = 0;
+            if (r < io.n_src && (!io.known || io.known[r])) {
                 load_group_bytes(io.src + (uint64_t)(io.row_map ? io.row_map[r] : r) * io.L, g0 + g, io.L, w);
                 bitslice16(w);
-                if (!io.in_scale) {
-#pragma unroll
-                    for (int q = 0; q < 16; q++) acc[q] = w[q];
-                }
             }
-            if (io.in_scale) mul16_lanes(have ? io.in_scale[r] : 0u, acc, w);
-            if (!valid) continue;
 #pragma unroll
             for (int q = 0; q < 4; q++)
-                *reinterpret_cast<uint4*>(piece(i, q, g)) =
-                    make_uint4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+                *reinterpret_cast<uint4*>(piece(i, q, g)) = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+        }
+        if (io.early_read) pdl_wait();
+        // times the locator value of each row (the previous kernel's output);
+        // every thread rescales the elements it stored
+        if (io.in_scale) {
+            for (uint32_t x0 = tid - lane; x0 < rows * gn; x0 += blockDim.x) {
+                const uint32_t x = x0 + lane;
+                const bool valid = x < rows * gn;
+                const uint32_t g = valid ? x % gn : 0u, i = valid ? x / gn : 0u;
+                const uint32_t r = row_of(i);
+                const bool have = valid && r < io.n_src && (!io.known || io.known[r]);
+                uint32_t w[16], acc[16];
+#pragma unroll
+                for (int q = 0; q < 16; q++) acc[q] = 0, w[q] = 0;
+                if (valid) {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const uint4 v = *reinterpret_cast<const uint4*>(piece(i, q, g));
+                        w[4 * q] = v.x, w[4 * q + 1] = v.y, w[4 * q + 2] = v.z, w[4 * q + 3] = v.w;
+                    }
+                }
+                mul16_lanes(have ? io.in_scale[r] : 0u, acc, w);
+                if (!valid) continue;
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    *reinterpret_cast<uint4*>(piece(i, q, g)) =
+                        make_uint4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+            }
         }
     } else {
+        pdl_wait();
         // the copies are asynchronous, so every thread has all of its loads in flight
         for (uint32_t x = tid; x < rows * gn * 4; x += blockDim.x) {
             const uint32_t q = x & 3, g = (x >> 2) % gn, i = (x >> 2) / gn;
@@ -895,9 +922,6 @@ __device__ __forceinline__ uint32_t lmul(const uint16_t* lg, const uint16_t* ex,
     uint32_t e = (uint32_t)lg[a] + lg[b];
     return ex[e >= kMult ? e - kMult : e];
 }
-__device__ __forceinline__ uint32_t linv(const uint16_t* lg, const uint16_t* ex, uint32_t a) {
-    return ex[(kMult - lg[a]) % kMult];
-}
 
 // gen[t*k + i] = G[t][i] for the r received repairs at evaluation points rep[t].
 __global__ void targeted_gen_kernel(const uint16_t* sys_values, const uint16_t* sys_derivs, const uint16_t* lg,
@@ -913,42 +937,6 @@ __global__ void targeted_gen_kernel(const uint16_t* sys_values, const uint16_t* 
 
 // One thread: invert A (r x r, GF(2^16) Gauss-Jordan; invertible for every
 // supported pattern) into inv[s*r + t] = (A^-1)[s][t].
-__global__ void targeted_invert_kernel(const uint16_t* gen, const uint16_t* missing, uint32_t r, uint32_t k,
-                                       const uint16_t* lg, const uint16_t* ex, uint16_t* inv, int32_t* status) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    uint32_t a[kTargetedMax][2 * kTargetedMax];
-    for (uint32_t t = 0; t < r; t++)
-        for (uint32_t s = 0; s < r; s++) {
-            a[t][s] = gen[(size_t)t * k + missing[s]];
-            a[t][r + s] = t == s;
-        }
-    bool ok = true;
-    for (uint32_t col = 0; col < r && ok; col++) {
-        uint32_t piv = col;
-        while (piv < r && !a[piv][col]) piv++;
-        if (piv == r) {
-            ok = false;
-            break;
-        }
-        if (piv != col)
-            for (uint32_t q = 0; q < 2 * r; q++) {
-                const uint32_t tmp = a[col][q];
-                a[col][q] = a[piv][q];
-                a[piv][q] = tmp;
-            }
-        const uint32_t pinv = linv(lg, ex, a[col][col]);
-        for (uint32_t q = 0; q < 2 * r; q++) a[col][q] = lmul(lg, ex, a[col][q], pinv);
-        for (uint32_t t = 0; t < r; t++) {
-            if (t == col || !a[t][col]) continue;
-            const uint32_t f = a[t][col];
-            for (uint32_t q = 0; q < 2 * r; q++) a[t][q] ^= lmul(lg, ex, f, a[col][q]);
-        }
-    }
-    if (!ok && status) atomicCAS(status, 0, SCRS_DECODE_INSUFFICIENT_RANK);
-    for (uint32_t s = 0; s < r; s++)
-        for (uint32_t t = 0; t < r; t++) inv[s * r + t] = ok ? (uint16_t)a[s][r + t] : 0;
-}
-
 // Fused coefficients, rows 0..r-1 the received repairs (A^-1 columns), rows
 // r.. the present data rows: row z, output s = sum_t (A^-1)[s][t] G[t][present[z]].
 __global__ void targeted_fuse_kernel(const uint16_t* gen, const uint16_t* inv_g, const uint16_t* present, uint32_t r,
@@ -1013,6 +1001,11 @@ int32_t AfftCodec::init(uint64_t k_, uint64_t m_, uint64_t L_, scrs_error* err) 
                             sys_values.as<uint16_t>(), sys_derivs.as<uint16_t>(), 0, err);
     if (r) return r;
     SCRS_CUDA(cudaStreamSynchronize(0));  // the locators ran on the legacy stream
+    // host copies for the targeted decode's r x r solve
+    h_sys_values.resize(ts);
+    h_sys_derivs.resize(ts);
+    SCRS_CUDA(cudaMemcpy(h_sys_values.data(), sys_values.p, ts * 2, cudaMemcpyDeviceToHost));
+    SCRS_CUDA(cudaMemcpy(h_sys_derivs.data(), sys_derivs.p, ts * 2, cudaMemcpyDeviceToHost));
     return SCRS_OK;
 }
 
@@ -1186,6 +1179,7 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
     in.in_scale = ws.values.as<uint16_t>();
     in.n_src = (uint32_t)ts;
     in.L = L;
+    in.early_read = 1;  // the previous kernel is the locator
     SCRS_CUDA(run_transform(ws.work0.as<uint8_t>(), G, (int)log_ts, factors.as<uint16_t>(), false, st, 1, in));
     SCRS_CUDA(launch_derivative(ws.work0.as<uint8_t>(), ws.work1.as<uint8_t>(), (uint32_t)ts, G, (int)log_ts,
                                 deriv_factors, st));
@@ -1224,6 +1218,34 @@ int32_t AfftCodec::targeted_lists(const uint8_t* have, AfftWorkspace& ws, scrs_e
     auto payload_row = [&](uint32_t w) { return row_map ? row_map[w] : (uint16_t)w; };
     for (uint32_t t = 0; t < nm; t++) in_rows[t] = payload_row(rep[t]), out_rows[t] = miss[t], mis[t] = miss[t];
     for (uint32_t z = 0; z < np; z++) in_rows[nm + z] = payload_row(pres[z]), prs[z] = pres[z];
+    // A[t][s] = G[t][missing s], G[t][i] = L_S(e_t) / ((e_t + i) L_S'(i))
+    // (generator_row, decoder.rs:600-619), inverted by Gauss-Jordan over
+    // GF(2^16) (invert_square_into, decoder.rs:619-670): r <= 5, so on the
+    // host, into the list area after the present rows (uploaded with it).
+    uint16_t a[kTargetedMax][2 * kTargetedMax];
+    for (uint32_t t = 0; t < nm; t++)
+        for (uint32_t s = 0; s < nm; s++) {
+            const uint16_t d = hf::mul16((uint16_t)(rep[t] ^ miss[s]), h_sys_derivs[miss[s]]);
+            a[t][s] = hf::mul16(h_sys_values[rep[t]], hf::inv16(d));
+            a[t][nm + s] = t == s;
+        }
+    for (uint32_t col = 0; col < nm; col++) {
+        uint32_t piv = col;
+        while (piv < nm && !a[piv][col]) piv++;
+        if (piv == nm) return set_err(err, SCRS_DECODE_INSUFFICIENT_RANK, k, k - 1);
+        if (piv != col)
+            for (uint32_t q = 0; q < 2 * nm; q++) std::swap(a[col][q], a[piv][q]);
+        const uint16_t pinv = hf::inv16(a[col][col]);
+        for (uint32_t q = 0; q < 2 * nm; q++) a[col][q] = hf::mul16(a[col][q], pinv);
+        for (uint32_t t = 0; t < nm; t++) {
+            if (t == col || !a[t][col]) continue;
+            const uint16_t f = a[t][col];
+            for (uint32_t q = 0; q < 2 * nm; q++) a[t][q] ^= hf::mul16(f, a[col][q]);
+        }
+    }
+    uint16_t* inv = prs + k;
+    for (uint32_t s = 0; s < nm; s++)
+        for (uint32_t t = 0; t < nm; t++) inv[s * nm + t] = a[s][nm + t];
     return SCRS_OK;
 }
 
@@ -1239,9 +1261,7 @@ int32_t AfftCodec::decode_targeted(const uint8_t* d_payloads, uint8_t* d_out, Af
     targeted_gen_kernel<<<grid_for((uint64_t)nm * k, 256), 256, 0, st>>>(
         sys_values.as<uint16_t>(), sys_derivs.as<uint16_t>(), lg, ex, d_rep, nm, (uint32_t)k, ws.tgen.as<uint16_t>());
     SCRS_CUDA(cudaGetLastError());
-    uint16_t* d_inv = const_cast<uint16_t*>(d_prs) + k;  // r*r entries after the present list
-    targeted_invert_kernel<<<1, 32, 0, st>>>(ws.tgen.as<uint16_t>(), d_mis, nm, (uint32_t)k, lg, ex, d_inv, status);
-    SCRS_CUDA(cudaGetLastError());
+    const uint16_t* d_inv = d_prs + k;  // r*r entries of A^-1 after the present list
     targeted_fuse_kernel<<<grid_for((uint64_t)k * nm, 256), 256, 0, st>>>(ws.tgen.as<uint16_t>(), d_inv, d_prs, nm,
                                                                          (uint32_t)k, lg, ex, ws.tcoef.as<uint16_t>());
     SCRS_CUDA(cudaGetLastError());

@@ -51,6 +51,7 @@ class AfftCodec {
     // Systematic locator L_S(x) = prod_{i<k}(x + i) (decoder.rs:256-266):
     // sys_values[e] = L_S(e) for e >= k, sys_derivs[i] = L_S'(i) for i < k.
     DevBuf sys_values, sys_derivs;
+    std::vector<uint16_t> h_sys_values, h_sys_derivs;  // host copies (targeted r x r solve)
 };
 
 class AfftWorkspace {

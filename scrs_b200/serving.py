@@ -34,6 +34,18 @@ class _Stats(C.Structure):
                 ("resident_bytes", C.c_uint64)]
 
 
+_COMPLETION_DTYPE = np.dtype([("ticket", np.uint64), ("tag", np.uint64), ("status", np.int32),
+                               ("reserved", np.int32), ("submit_ns", np.uint64), ("done_ns", np.uint64)])
+assert _COMPLETION_DTYPE.itemsize == C.sizeof(_Completion)
+
+
+@dataclass
+class Prepared:
+    """A request for ``Server.submit_prepared`` (keeps its index list alive)."""
+    req: _Request
+    indices: Optional[np.ndarray]
+
+
 @dataclass
 class Completion:
     ticket: int
@@ -107,6 +119,39 @@ class Server:
         err = _Error()
         self._lib.check(self._lib.lib.scrs_server_submit(self._ptr, C.byref(r), C.byref(t), C.byref(err)), err)
         return t.value
+
+    def prepare(self, op: int, engine, k: int, m: int, symbol_len: int, in_ptr: int, out_ptr: int,
+                indices: Optional[Sequence[int]] = None, tag: int = 0, stream=None) -> "Prepared":
+        """A request built once and submitted any number of times with
+        ``submit_prepared`` (the same buffers each time): the per-submit host
+        cost is one library call."""
+        arr = None if indices is None else np.ascontiguousarray(indices, dtype=np.uint64)
+        r = _Request(op, int(engine), k, m, symbol_len, in_ptr, out_ptr, None, tag, _stream_ptr(stream))
+        if arr is not None:
+            r.indices = arr.ctypes.data_as(C.POINTER(C.c_uint64))
+        return Prepared(r, arr)
+
+    def submit_prepared(self, p: "Prepared") -> int:
+        t = C.c_uint64()
+        err = _Error()
+        self._lib.check(self._lib.lib.scrs_server_submit(self._ptr, C.byref(p.req), C.byref(t), C.byref(err)), err)
+        return t.value
+
+    def progress_arrays(self):
+        """As ``progress``, the completions as numpy arrays (tag, status,
+        submit_ns, done_ns) instead of one object each."""
+        chunks = []
+        while True:
+            n = C.c_uint32()
+            err = _Error()
+            self._lib.check(self._lib.lib.scrs_server_progress(self._ptr, self._buf, len(self._buf), C.byref(n),
+                                                               C.byref(err)), err)
+            if n.value:
+                chunks.append(np.frombuffer(self._buf, dtype=_COMPLETION_DTYPE, count=n.value).copy())
+            if n.value < len(self._buf):
+                break
+        done = np.concatenate(chunks) if chunks else np.zeros(0, _COMPLETION_DTYPE)
+        return done["tag"], done["status"], done["submit_ns"], done["done_ns"]
 
     def progress(self) -> List[Completion]:
         out = []

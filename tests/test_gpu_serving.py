@@ -78,6 +78,37 @@ def test_results_alone_and_in_mix_match(gpu, oracle):
     srv.close()
 
 
+def test_prepared_requests_and_array_completions(gpu, oracle):
+    """Requests built once (Server.prepare) and submitted twice give the same
+    bytes as the oracle, and progress_arrays reports every completion once
+    with its tag, a zero status and ordered timestamps."""
+    torch = pytest.importorskip("torch")
+    from scrs_b200.serving import Server
+
+    reqs = make_requests(torch, oracle, seed=23)[:12]
+    srv = Server(gpu.lib, 1 << 30, slots=4)
+    outs = [torch.full((len(r[-1]),), 0xAB, dtype=torch.uint8, device="cuda") for r in reqs]
+    prepared = [srv.prepare(op, engine, k, m, L, d_in.data_ptr(), outs[q].data_ptr(), idx, tag=q)
+                for q, (op, engine, k, m, L, d_in, idx, _) in enumerate(reqs)]
+    for round_ in range(2):
+        for p in prepared:
+            srv.submit_prepared(p)
+        tags, status, sub_ns, done_ns = [], [], [], []
+        while srv.pending:
+            t, st, a, b = srv.progress_arrays()
+            tags.extend(t.tolist())
+            status.extend(st.tolist())
+            sub_ns.extend(a.tolist())
+            done_ns.extend(b.tolist())
+        assert sorted(tags) == list(range(len(reqs)))
+        assert all(v == 0 for v in status)
+        assert all(b >= a for a, b in zip(sub_ns, done_ns))
+        torch.cuda.synchronize()
+        for q, r in enumerate(reqs):
+            assert np.array_equal(outs[q].cpu().numpy(), r[-1]), (round_, q)
+    srv.close()
+
+
 def test_small_budget_queues_and_completes(gpu, oracle):
     torch = pytest.importorskip("torch")
     from scrs_b200.serving import Server
