@@ -237,6 +237,24 @@ def test_afft_cfg3b_shape(gpu, oracle):
     assert np.array_equal(batch_decode(gpu, p, word, few), data)
 
 
+
+@pytest.mark.parametrize("k,m,L", [(1500, 700, 130), (1200, 300, 96), (10000, 3000, 64), (8192, 100, 64),
+                                   (16384, 16384, 32), (2000, 48, 4096)])
+def test_afft_mid_size_shapes(gpu, oracle, k, m, L):
+    """Transforms of 2^11 to 2^15 points: the power-of-two encode (k = 8192,
+    16384), the general-k encode and the full decode at each transform size,
+    with odd symbol lengths and up to 64 column groups: repairs equal the
+    oracle's and a random k of the n symbols give the data back."""
+    p = gpu.resolve(Engine.AFFT, k, m, L)
+    data = gfpy.rng_bytes(k * L, 0xC1 + k + m)
+    word = encode_word(gpu, p, data)
+    exp = np.zeros(m * L, np.uint8)
+    oracle.batch_encoder(p).encode_into(data, exp)
+    assert np.array_equal(np.concatenate(word[k:]), exp)
+    sel = np.random.default_rng(k + m).permutation(k + m)[:k].tolist()
+    assert np.array_equal(batch_decode(gpu, p, word, sel), data)
+    assert np.array_equal(lazy_decode(gpu, p, word, sel), data)
+
 @pytest.mark.parametrize("k,m,L", [(4096, 64, 1024), (1000, 24, 258), (37, 11, 6), (2048, 8, 4096)])
 def test_afft_targeted_few_erasures(gpu, oracle, k, m, L):
     """r <= 5 missing data symbols take the targeted path (one coefficient
