@@ -31,6 +31,9 @@
 #include <new>
 #include <thread>
 #include <tuple>
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
 
 #include "host_field.h"
 #include "jit.h"
@@ -853,6 +856,39 @@ int32_t enqueue_batch(scrs_stripe_batch* b, cudaStream_t st, scrs_error* err) {
     return SCRS_OK;
 }
 
+// Row copy on a host worker that leaves the destination out of the caches:
+// the rows are 4 KiB or so, below the size where memcpy itself switches to
+// non-temporal stores, and a regular store first reads the destination line
+// from host memory, which the copy engines are reading and writing at the
+// same time.  16-byte aligned rows of whole 16-byte units take the streaming
+// stores (the caller fences once after its copies); anything else memcpy.
+void copy_row_streaming(uint8_t* dst, const uint8_t* src, size_t bytes) {
+#if defined(__SSE2__)
+    if (((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src) | bytes) & 15) == 0) {
+        __m128i* d = reinterpret_cast<__m128i*>(dst);
+        const __m128i* s = reinterpret_cast<const __m128i*>(src);
+        size_t n = bytes / 16, i = 0;
+        for (; i + 4 <= n; i += 4) {
+            const __m128i a = _mm_load_si128(s + i), b = _mm_load_si128(s + i + 1);
+            const __m128i c = _mm_load_si128(s + i + 2), e = _mm_load_si128(s + i + 3);
+            _mm_stream_si128(d + i, a);
+            _mm_stream_si128(d + i + 1, b);
+            _mm_stream_si128(d + i + 2, c);
+            _mm_stream_si128(d + i + 3, e);
+        }
+        for (; i < n; i++) _mm_stream_si128(d + i, _mm_load_si128(s + i));
+        return;
+    }
+#endif
+    memcpy(dst, src, bytes);
+}
+
+void fence_streaming_stores() {
+#if defined(__SSE2__)
+    _mm_sfence();
+#endif
+}
+
 // The host side of a host-buffer run's decode stripes, on the worker
 // threads: first every present row (caller's input row -> output row), then
 // piece by piece, once the piece's device->host copies are done (its event,
@@ -869,7 +905,7 @@ int32_t host_copies(scrs_stripe_batch* b, bool pieces_done, scrs_error* err) {
         };
         const auto pr = share(0, b->present_copies.size(), w);
         for (size_t i = pr.first; i < pr.second; i++)
-            memcpy(b->present_copies[i].dst, b->present_copies[i].src, b->present_copies[i].bytes);
+            copy_row_streaming(b->present_copies[i].dst, b->present_copies[i].src, b->present_copies[i].bytes);
         for (size_t q = 0; q + 1 < b->missing_at.size(); q++) {
             const auto mr = share(b->missing_at[q], b->missing_at[q + 1], w);
             if (mr.first == mr.second) continue;
@@ -877,12 +913,14 @@ int32_t host_copies(scrs_stripe_batch* b, bool pieces_done, scrs_error* err) {
                 const cudaError_t e = cudaEventSynchronize(b->events[2 + 2 * kMaxPieces + q]);
                 if (e != cudaSuccess) {
                     failed.store((int)e);
+                    fence_streaming_stores();
                     return;
                 }
             }
             for (size_t i = mr.first; i < mr.second; i++)
-                memcpy(b->missing_copies[i].dst, b->missing_copies[i].src, b->missing_copies[i].bytes);
+                copy_row_streaming(b->missing_copies[i].dst, b->missing_copies[i].src, b->missing_copies[i].bytes);
         }
+        fence_streaming_stores();  // the stores are visible to the caller once run() returns
     };
     b->pool->run(work);
     if (failed.load()) return set_err(err, SCRS_ERR_CUDA, (uint64_t)failed.load(), __LINE__);
