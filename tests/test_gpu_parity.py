@@ -4,7 +4,7 @@ library and through the oracle's identical ABI on the same seeded inputs."""
 import numpy as np
 import pytest
 
-from scrs_b200.api import DEPENDENT, DecodeError, EncodeError, Engine, PushOutcome
+from scrs_b200.api import DEPENDENT, ConfigError, DecodeError, EncodeError, Engine, PushOutcome
 
 import gfpy
 from scenarios import (batch_decode, deterministic_subsets, device_stripes, encode_word, k_subsets, lazy_decode,
@@ -28,7 +28,13 @@ def words_equal(a, b):
                                    (10, 4, 1000), (40, 16, 65536), (33, 3, 1025), (200, 56, 256)])
 def test_gf256_encode_matches_oracle(gpu, oracle, engine, k, m, L):
     if engine == Engine.GOOD_CAUCHY and k + m > 255:
-        pytest.skip("Good Cauchy capacity is 255")
+        # Good Cauchy holds at most 255 symbols: both sides refuse the profile alike
+        with pytest.raises(ConfigError) as got_err:
+            gpu.resolve(engine, k, m, L)
+        with pytest.raises(ConfigError) as exp_err:
+            oracle.resolve(engine, k, m, L)
+        assert got_err.value.code == 102 and got_err.value == exp_err.value
+        return
     p = gpu.resolve(engine, k, m, L)
     data = gfpy.rng_bytes(k * L, k * 1000 + m)
     got = np.zeros(m * L, np.uint8)
