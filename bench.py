@@ -1167,9 +1167,9 @@ def run_ours(args, world, rank, local):
             "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if
             peak_kind == "measured" else "fallback 6650 GB/s",
             "traffic": round(ratio * algorithmic_bytes()) if ratio else None,
-            "traffic_source": ("DRAM bytes per algorithmic byte of an ncu capture at 8192+8192 stripes "
-                               "(profiles/gf256_mxk_cfg1_ncu.md) times this launch's algorithmic bytes: the "
-                               "full-size launch is too large to capture; traffic grows with the stripes"),
+            "traffic_source": ("DRAM bytes per algorithmic byte of a 1-pass ncu capture of the full-size "
+                               "65536+65536-stripe launches (dram__bytes_read.sum + dram__bytes_write.sum, "
+                               "profiles/gf256_mxk_cfg1_ncu.md) times this launch's algorithmic bytes"),
             "kernel": ("persistent drain: scrs_spec_drain (encode stripes, kernel specialised to the matrix) "
                        "then mxk_kernel<0, 7> (decode stripes; rows 16-byte aligned, whole 2 KiB chunks, "
                        "one segment)" if enc_spec else "mxk_kernel<0, 7> persistent drain"),
