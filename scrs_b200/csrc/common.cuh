@@ -148,7 +148,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 }
 
 // 1-D bulk copy global -> shared, completing on `bar` (both addresses 16-byte
-// aligned, bytes a multiple of 16).  No cluster multicast.
+// aligned, bytes a multiple of 16), into this CTA's shared memory only.
 __device__ __forceinline__ void tma_load_1d(void* smem_dst, const void* gmem_src, uint32_t bytes,
                                             uint64_t* bar) {
     asm volatile(

@@ -4,7 +4,7 @@
 // owns 64 bytes of each row (two sets of 8 GF(256) bit planes, or one set of
 // 16 GF(2^16) planes).
 // For each segment of up to 16 input rows:
-//   1. one thread issues a TMA bulk copy (cp.async.bulk, no multicast) per
+//   1. one thread issues a TMA bulk copy (cp.async.bulk, into this CTA only) per
 //      input row into shared memory; all threads wait on the stage's mbarrier;
 //   2. each warp bit-slices its share of the staged rows in place (and writes
 //      decode's present rows straight through to the output);
