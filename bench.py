@@ -1223,7 +1223,9 @@ def run_ours(args, world, rank, local):
                        "only their missing rows, their present rows are copied host-side while the GPU runs)"}
         launches += hb.last_launches * n_e2e
     extras = {}
-    if rank == 0 and not args.no_extras:
+    # the extras and the CPU baseline are single-GPU figures: taken at N = 1
+    # only, so a multi-GPU run holds its GPUs for the headline alone
+    if rank == 0 and world == 1 and not args.no_extras:
         cpu_legs = None if args.no_cpu else Cpu()
         for name, fn in EXTRAS.items():
             try:
@@ -1232,7 +1234,7 @@ def run_ours(args, world, rank, local):
                 extras[name] = {"error": repr(ex)[:300]}
     if rank != 0:
         return
-    cpu = None if args.no_cpu else cpu_baseline()
+    cpu = None if args.no_cpu or world > 1 else cpu_baseline()
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
