@@ -378,10 +378,15 @@ __global__ void __launch_bounds__(128) derivative_kernel(const uint8_t* in, uint
 // dst row rows[t] = src row (row_map ? row_map[rows[t]] : rows[t]), L bytes
 // each, in units of `unit` bytes (16 when both bases are 16-byte aligned and
 // L is a multiple of 16, else 1).
+// With `chain` (launched with programmatic dependent launch right after the
+// decode's locator, whose output it does not read) the copy runs beside the
+// locator and waits for it only before exiting, so the next kernel's wait on
+// this one also covers the locator.
 template <int kUnit>
 __global__ void copy_rows_kernel(const uint8_t* src, uint8_t* dst, uint64_t L, const uint16_t* rows,
-                                 uint32_t count, const uint16_t* row_map) {
+                                 uint32_t count, const uint16_t* row_map, int chain) {
     using U = typename std::conditional<kUnit == 16, uint4, uint8_t>::type;
+    if (chain) pdl_trigger();
     const uint64_t per = L / kUnit;
     const uint64_t total = (uint64_t)count * per;
     for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < total;
@@ -391,6 +396,7 @@ __global__ void copy_rows_kernel(const uint8_t* src, uint8_t* dst, uint64_t L, c
         const uint64_t s = row_map ? row_map[r] : r;
         reinterpret_cast<U*>(dst + r * L)[q] = reinterpret_cast<const U*>(src + s * L)[q];
     }
+    if (chain) pdl_wait();
 }
 
 // ---- transform passes ---------------------------------------------------------
@@ -444,9 +450,10 @@ struct PassIo {
     const uint16_t* exp16;
     uint64_t L;
     // the slice's byte rows, row map and known mask were complete before the
-    // previous kernel on the stream started (the decode's locator, itself
-    // launched without programmatic serialisation): the first pass reads them
-    // before waiting on that kernel, and waits only for in_scale
+    // decode's locator started (it is launched without programmatic
+    // serialisation, after their upload): the first pass reads them before
+    // waiting on the kernel before it (the locator, or the present-row copy
+    // chained after it), and waits only for in_scale
     int32_t early_read;
 };
 
@@ -1156,22 +1163,34 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
     const uint16_t* d_pres = reinterpret_cast<const uint16_t*>(dev) + k;
     const uint16_t* d_map = row_map ? reinterpret_cast<const uint16_t*>(dev + ws.off_map) : nullptr;
     const uint8_t* d_known = dev + ws.off_known;
-    if (np) {
+    // the present data rows, straight from the payloads into the output
+    auto copy_present = [&](int chain) -> cudaError_t {
+        if (!np) return cudaSuccess;
         const bool vec = L % 16 == 0 && (reinterpret_cast<uintptr_t>(d_payloads) & 15) == 0 &&
                          (reinterpret_cast<uintptr_t>(d_out) & 15) == 0;
-        if (vec)
-            copy_rows_kernel<16><<<grid_for((uint64_t)np * (L / 16), 256), 256, 0, st>>>(d_payloads, d_out, L,
-                                                                                            d_pres, np, d_map);
-        else
-            copy_rows_kernel<1><<<grid_for((uint64_t)np * L, 256), 256, 0, st>>>(d_payloads, d_out, L, d_pres, np,
-                                                                                   d_map);
-        SCRS_CUDA(cudaGetLastError());
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(vec ? grid_for((uint64_t)np * (L / 16), 256) : grid_for((uint64_t)np * L, 256));
+        cfg.blockDim = dim3(256);
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = chain ? 1 : 0;
+        return vec ? cudaLaunchKernelEx(&cfg, copy_rows_kernel<16>, d_payloads, d_out, L, d_pres, np, d_map, chain)
+                   : cudaLaunchKernelEx(&cfg, copy_rows_kernel<1>, d_payloads, d_out, L, d_pres, np, d_map, chain);
+    };
+    if (nm == 0 || targeted) {
+        SCRS_CUDA(copy_present(0));
+        if (nm == 0) return SCRS_OK;
+        return decode_targeted(d_payloads, d_out, ws, status, st, err, nm);
     }
-    if (nm == 0) return SCRS_OK;
-    if (targeted) return decode_targeted(d_payloads, d_out, ws, status, st, err, nm);
     int32_t r = afft_locator_device(d_known, (uint32_t)ts, log_walsh.as<uint32_t>(), ws.wht_a.as<uint32_t>(),
                                     ws.values.as<uint16_t>(), ws.derivs.as<uint16_t>(), st, err);
     if (r) return r;
+    // the copy runs beside the locator (it reads none of its output) and
+    // exits after it, so the first pass's wait covers both
+    SCRS_CUDA(copy_present(1));
     PassIo in{};
     in.src = d_payloads;
     in.known = d_known;
@@ -1179,7 +1198,7 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
     in.in_scale = ws.values.as<uint16_t>();
     in.n_src = (uint32_t)ts;
     in.L = L;
-    in.early_read = 1;  // the previous kernel is the locator
+    in.early_read = 1;  // the previous kernels are the locator and the chained copy
     SCRS_CUDA(run_transform(ws.work0.as<uint8_t>(), G, (int)log_ts, factors.as<uint16_t>(), false, st, 1, in));
     SCRS_CUDA(launch_derivative(ws.work0.as<uint8_t>(), ws.work1.as<uint8_t>(), (uint32_t)ts, G, (int)log_ts,
                                 deriv_factors, st));
