@@ -116,13 +116,6 @@ __device__ __forceinline__ uint32_t add_mod(uint32_t a, uint32_t b) {
 }
 __device__ __forceinline__ uint32_t sub_mod(uint32_t a, uint32_t b) { return a >= b ? a - b : a + kMult - b; }
 
-// Programmatic dependent launch: a kernel launched with the programmatic
-// stream serialization attribute may start while the kernel before it on the
-// stream is still running.  It reads nothing that kernel writes before
-// pdl_wait(), which returns once that kernel has completed and its writes are
-// visible; pdl_trigger() lets the next such kernel start its own prologue.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // ---- erasure locator (decoder.rs:672-755) ----------------------------------------
 // log L(x) for every point x is a Walsh-Hadamard transform (mod 65535) of the
@@ -931,8 +924,11 @@ __device__ __forceinline__ uint32_t lmul(const uint16_t* lg, const uint16_t* ex,
 }
 
 // gen[t*k + i] = G[t][i] for the r received repairs at evaluation points rep[t].
+// Launched chained after the present-row copy, whose output it does not read:
+// it runs beside it and waits for it only before exiting.
 __global__ void targeted_gen_kernel(const uint16_t* sys_values, const uint16_t* sys_derivs, const uint16_t* lg,
                                     const uint16_t* ex, const uint16_t* rep, uint32_t r, uint32_t k, uint16_t* gen) {
+    pdl_trigger();
     for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < (uint64_t)r * k;
          x += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t t = (uint32_t)(x / k), i = (uint32_t)(x - (uint64_t)t * k);
@@ -940,16 +936,17 @@ __global__ void targeted_gen_kernel(const uint16_t* sys_values, const uint16_t* 
         uint32_t lv = (uint32_t)lg[sys_values[e]] + 2 * kMult - lg[e ^ i] - lg[sys_derivs[i]];
         gen[x] = ex[lv % kMult];
     }
+    pdl_wait();
 }
 
-// One thread: invert A (r x r, GF(2^16) Gauss-Jordan; invertible for every
-// supported pattern) into inv[s*r + t] = (A^-1)[s][t].
 // Fused coefficients, rows 0..r-1 the received repairs (A^-1 columns), rows
 // r.. the present data rows: row z, output s = sum_t (A^-1)[s][t] G[t][present[z]].
 __global__ void targeted_fuse_kernel(const uint16_t* gen, const uint16_t* inv_g, const uint16_t* present, uint32_t r,
                                      uint32_t k, const uint16_t* lg, const uint16_t* ex, uint16_t* coef) {
     __shared__ uint32_t inv[kTargetedMax * kTargetedMax];
-    for (uint32_t x = threadIdx.x; x < r * r; x += blockDim.x) inv[x] = inv_g[x];
+    pdl_trigger();
+    for (uint32_t x = threadIdx.x; x < r * r; x += blockDim.x) inv[x] = inv_g[x];  // uploaded, not computed
+    pdl_wait();  // gen is the previous kernel's output
     __syncthreads();
     for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < (uint64_t)k * r;
          x += (uint64_t)gridDim.x * blockDim.x) {
@@ -1164,7 +1161,9 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
     const uint16_t* d_map = row_map ? reinterpret_cast<const uint16_t*>(dev + ws.off_map) : nullptr;
     const uint8_t* d_known = dev + ws.off_known;
     // the present data rows, straight from the payloads into the output
-    auto copy_present = [&](int chain) -> cudaError_t {
+    // chain: trigger the next kernel at once and wait for the previous one
+    // before exiting; attr: launched with programmatic dependent launch
+    auto copy_present = [&](int chain, bool attr_on) -> cudaError_t {
         if (!np) return cudaSuccess;
         const bool vec = L % 16 == 0 && (reinterpret_cast<uintptr_t>(d_payloads) & 15) == 0 &&
                          (reinterpret_cast<uintptr_t>(d_out) & 15) == 0;
@@ -1176,21 +1175,26 @@ int32_t AfftCodec::decode(const uint8_t* d_payloads, const uint8_t* have, uint8_
         attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
         attr[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
-        cfg.numAttrs = chain ? 1 : 0;
+        cfg.numAttrs = attr_on ? 1 : 0;
         return vec ? cudaLaunchKernelEx(&cfg, copy_rows_kernel<16>, d_payloads, d_out, L, d_pres, np, d_map, chain)
                    : cudaLaunchKernelEx(&cfg, copy_rows_kernel<1>, d_payloads, d_out, L, d_pres, np, d_map, chain);
     };
-    if (nm == 0 || targeted) {
-        SCRS_CUDA(copy_present(0));
-        if (nm == 0) return SCRS_OK;
-        return decode_targeted(d_payloads, d_out, ws, status, st, err, nm);
+    if (nm == 0) {
+        SCRS_CUDA(copy_present(0, false));
+        return SCRS_OK;
+    }
+    if (targeted) {
+        // after the upload (a copy, not a kernel): launched plainly, it lets
+        // the targeted kernels chained after it start beside it
+        SCRS_CUDA(copy_present(np ? 1 : 0, false));
+        return decode_targeted(d_payloads, d_out, ws, status, st, err, nm, np > 0);
     }
     int32_t r = afft_locator_device(d_known, (uint32_t)ts, log_walsh.as<uint32_t>(), ws.wht_a.as<uint32_t>(),
                                     ws.values.as<uint16_t>(), ws.derivs.as<uint16_t>(), st, err);
     if (r) return r;
     // the copy runs beside the locator (it reads none of its output) and
     // exits after it, so the first pass's wait covers both
-    SCRS_CUDA(copy_present(1));
+    SCRS_CUDA(copy_present(1, true));
     PassIo in{};
     in.src = d_payloads;
     in.known = d_known;
@@ -1268,8 +1272,12 @@ int32_t AfftCodec::targeted_lists(const uint8_t* have, AfftWorkspace& ws, scrs_e
     return SCRS_OK;
 }
 
+// The launches are chained (programmatic dependent launch): each kernel may
+// start while the one before it runs, reads that kernel's output only after
+// waiting for it, and has waited for it by the time it exits, so the last
+// one's completion covers them all.
 int32_t AfftCodec::decode_targeted(const uint8_t* d_payloads, uint8_t* d_out, AfftWorkspace& ws, int32_t* status,
-                                   cudaStream_t st, scrs_error* err, uint32_t nm) const {
+                                   cudaStream_t st, scrs_error* err, uint32_t nm, bool after_copy) const {
     const uint16_t *lg, *ex;
     SCRS_CUDA(log16_tables(&lg, &ex));
     const uint16_t* d_in_rows = reinterpret_cast<const uint16_t*>(ws.up.as<uint8_t>() + ws.off_lists);
@@ -1277,13 +1285,23 @@ int32_t AfftCodec::decode_targeted(const uint8_t* d_payloads, uint8_t* d_out, Af
     const uint16_t* d_rep = d_out_rows + kTargetedMax;
     const uint16_t* d_mis = d_rep + kTargetedMax;
     const uint16_t* d_prs = d_mis + kTargetedMax;
-    targeted_gen_kernel<<<grid_for((uint64_t)nm * k, 256), 256, 0, st>>>(
-        sys_values.as<uint16_t>(), sys_derivs.as<uint16_t>(), lg, ex, d_rep, nm, (uint32_t)k, ws.tgen.as<uint16_t>());
-    SCRS_CUDA(cudaGetLastError());
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cfg.attrs = attr;
+    // after the upload alone (a copy, not a kernel) the first launch is plain
+    cfg.numAttrs = after_copy ? 1 : 0;
+    cfg.gridDim = dim3(grid_for((uint64_t)nm * k, 256));
+    SCRS_CUDA(cudaLaunchKernelEx(&cfg, targeted_gen_kernel, sys_values.as<uint16_t>(), sys_derivs.as<uint16_t>(), lg,
+                                 ex, d_rep, nm, (uint32_t)k, ws.tgen.as<uint16_t>()));
     const uint16_t* d_inv = d_prs + k;  // r*r entries of A^-1 after the present list
-    targeted_fuse_kernel<<<grid_for((uint64_t)k * nm, 256), 256, 0, st>>>(ws.tgen.as<uint16_t>(), d_inv, d_prs, nm,
-                                                                         (uint32_t)k, lg, ex, ws.tcoef.as<uint16_t>());
-    SCRS_CUDA(cudaGetLastError());
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(grid_for((uint64_t)k * nm, 256));
+    SCRS_CUDA(cudaLaunchKernelEx(&cfg, targeted_fuse_kernel, (const uint16_t*)ws.tgen.as<uint16_t>(), d_inv, d_prs,
+                                 nm, (uint32_t)k, lg, ex, ws.tcoef.as<uint16_t>()));
     MxkTask T{};
     T.in = d_payloads;
     T.out = d_out;
@@ -1300,7 +1318,7 @@ int32_t AfftCodec::decode_targeted(const uint8_t* d_payloads, uint8_t* d_out, Af
     T.aligned = (L % 16 == 0 && aligned16(d_payloads) && aligned16(d_out)) ? 1u : 0u;
     // k inputs: the launch splits them over CTAs (input-split form) when the
     // output rows allow 4-byte atomics, else walks them per chunk
-    SCRS_CUDA(launch_mxk_single(T, 1, status, 0, st));
+    SCRS_CUDA(launch_mxk_single(T, 1, status, 0, st, /*chain=*/true));
     return SCRS_OK;
 }
 

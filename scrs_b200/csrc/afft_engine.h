@@ -39,8 +39,10 @@ class AfftCodec {
     size_t targeted_list_elems() const;
     int32_t targeted_lists(const uint8_t* have, AfftWorkspace& ws, scrs_error* err, const uint16_t* row_map,
                            const uint16_t* miss, uint32_t nm, const uint16_t* pres, uint32_t np) const;
+    // after_copy: the kernel before it on the stream is the present-row copy
+    // (its launches are chained after it, see afft.cu)
     int32_t decode_targeted(const uint8_t* d_payloads, uint8_t* d_out, AfftWorkspace& ws, int32_t* status,
-                            cudaStream_t st, scrs_error* err, uint32_t nm) const;
+                            cudaStream_t st, scrs_error* err, uint32_t nm, bool after_copy = false) const;
 
     uint64_t k = 0, m = 0, n = 0, L = 0, padded_k = 0, ts = 0;
     uint32_t log_ts = 0;

@@ -94,6 +94,15 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
+// Programmatic dependent launch: a kernel launched with the programmatic
+// stream serialization attribute may start while the kernel before it on the
+// stream is still running.  It reads nothing that kernel writes before
+// pdl_wait(), which returns once that kernel has completed and its writes are
+// visible (at once for a kernel launched without the attribute);
+// pdl_trigger() lets the next such kernel start its own prologue.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ void report_status(int32_t* status, int32_t code) {
     if (status) atomicCAS(status, 0, code);
 }

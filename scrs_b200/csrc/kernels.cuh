@@ -112,8 +112,12 @@ cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, ui
                              uint32_t* work_counter, int32_t* status, int seg_rows, int grid, cudaStream_t stream,
                              int shape = kShapeAny, int gf16 = 0);
 // One task by value; grid <= 0 means one CTA per row chunk (or the
-// input-split form for more than one segment of inputs, see below).
-cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream);
+// input-split form for more than one segment of inputs, see below).  `chain`:
+// the input-split form's launches use programmatic dependent launch, so they
+// may start while the kernel before them on the stream runs (they wait for it
+// before reading the coefficients); the single-kernel form ignores it.
+cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream,
+                              bool chain = false);
 cudaError_t launch_cauchy_plan_single(const CauchyPlanTask& task, int gf16, cudaStream_t stream);
 // Input-split form: inputs split into blocks over CTAs, partial sums XORed
 // (atomicXor) into the outputs, which the launch zeroes first unless the task

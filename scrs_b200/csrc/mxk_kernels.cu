@@ -351,14 +351,21 @@ __global__ void __launch_bounds__(kThreads, 8) mxk_single_kernel(const MxkTask T
 // with atomicXor (outputs zeroed beforehand unless accumulating), so all
 // input blocks run in parallel instead of one CTA walking every segment and
 // re-reading its partial sums.
+// With `chain` (programmatic dependent launch) the set-up overlaps the kernel
+// before, and the items start once it has completed (its coefficients and
+// zeroed outputs visible).
 template <int kGf16>
 __global__ void __launch_bounds__(kThreads, 8) mxk_ksplit_kernel(const MxkTask T, int32_t* status, int seg_cap,
-                                                                 uint32_t per) {
+                                                                 uint32_t per, int chain) {
     extern __shared__ __align__(128) uint8_t smem[];
     const SmemLayout S = layout<kGf16>(smem, seg_cap);
     if (threadIdx.x == 0) {
         mbar_init(S.bar, 1);
         fence_mbar_init();
+    }
+    if (chain) {
+        pdl_trigger();
+        pdl_wait();
     }
     __syncthreads();
     uint32_t phase = 0;
@@ -378,7 +385,11 @@ __global__ void __launch_bounds__(kThreads, 8) mxk_ksplit_kernel(const MxkTask T
 }
 
 // Zero the output rows of T (4-byte words; L % 4 == 0).
-__global__ void zero_out_rows_kernel(const MxkTask T) {
+// With `chain` (programmatic dependent launch after the kernel that builds the
+// task's coefficients) the zeroing runs beside that kernel and waits for it
+// only before exiting.
+__global__ void zero_out_rows_kernel(const MxkTask T, int chain) {
+    if (chain) pdl_trigger();
     const uint64_t words = T.L / 4;
     for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < (uint64_t)T.n_out * words;
          x += (uint64_t)gridDim.x * blockDim.x) {
@@ -386,6 +397,7 @@ __global__ void zero_out_rows_kernel(const MxkTask T) {
         const uint32_t r = T.out_rows ? T.out_rows[j] : j;
         reinterpret_cast<uint32_t*>(T.out + (uint64_t)r * T.out_stride)[x - (uint64_t)j * words] = 0;
     }
+    if (chain) pdl_wait();
 }
 
 // ---- bounded-wait self-test -------------------------------------------------
@@ -674,14 +686,24 @@ cudaError_t set_mxk_attrs() {
 // Input-split launch (see mxk_ksplit_kernel): outputs are zeroed first unless
 // the task accumulates; about four outputs per item.
 template <int kGf16>
-cudaError_t launch_ksplit_impl(const MxkTask& T, int32_t* status, cudaStream_t stream) {
+cudaError_t launch_ksplit_impl(const MxkTask& T, int32_t* status, cudaStream_t stream, bool chain = false) {
     using G = FieldGeom<kGf16>;
     cudaError_t ea = set_mxk_attrs<kGf16>();
     if (ea != cudaSuccess) return ea;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(kThreads);
+    cfg.stream = stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = chain ? 1 : 0;
     if (!T.accumulate && T.n_out) {
         const uint64_t words = (uint64_t)T.n_out * (T.L / 4);
-        zero_out_rows_kernel<<<(int)std::min<uint64_t>((words + 255) / 256, 148 * 16), 256, 0, stream>>>(T);
-        cudaError_t e = cudaGetLastError();
+        cudaLaunchConfig_t zc = cfg;
+        zc.gridDim = dim3((unsigned)std::min<uint64_t>((words + 255) / 256, 148 * 16));
+        zc.blockDim = dim3(256);
+        cudaError_t e = cudaLaunchKernelEx(&zc, zero_out_rows_kernel, T, (int)chain);
         if (e != cudaSuccess) return e;
     }
     const int seg_cap = std::max(1, std::min((int)T.n_in, G::kSeg));
@@ -689,8 +711,9 @@ cudaError_t launch_ksplit_impl(const MxkTask& T, int32_t* status, cudaStream_t s
     const uint32_t splits = T.n_out ? (T.n_out + per - 1) / per : 1;
     const uint64_t items = (uint64_t)T.n_items * splits * ((T.n_in + seg_cap - 1) / seg_cap);
     const int grid = (int)std::min<uint64_t>(items, 148u * 8u);
-    mxk_ksplit_kernel<kGf16><<<grid, kThreads, smem_bytes(kGf16, seg_cap), stream>>>(T, status, seg_cap, per);
-    return cudaGetLastError();
+    cfg.gridDim = dim3(grid);
+    cfg.dynamicSmemBytes = smem_bytes(kGf16, seg_cap);
+    return cudaLaunchKernelEx(&cfg, mxk_ksplit_kernel<kGf16>, T, status, seg_cap, per, (int)chain);
 }
 
 // Whether partial sums of T's outputs can be combined with 4-byte atomicXor.
@@ -699,14 +722,14 @@ bool ksplit_ok(const MxkTask& T) {
 }
 
 template <int kGf16>
-cudaError_t launch_single_impl(const MxkTask& T, int32_t* status, int grid, cudaStream_t stream) {
+cudaError_t launch_single_impl(const MxkTask& T, int32_t* status, int grid, cudaStream_t stream, bool chain) {
     using G = FieldGeom<kGf16>;
     if (T.n_items == 0 || (T.n_out == 0 && T.pass_rows == nullptr)) return cudaSuccess;
     cudaError_t e = set_mxk_attrs<kGf16>();
     if (e != cudaSuccess) return e;
     int seg_cap = std::max(1, std::min((int)T.n_in, G::kSeg));
     // More than one segment of inputs: split the inputs over CTAs instead.
-    if ((int)T.n_in > seg_cap && ksplit_ok(T)) return launch_ksplit_impl<kGf16>(T, status, stream);
+    if ((int)T.n_in > seg_cap && ksplit_ok(T)) return launch_ksplit_impl<kGf16>(T, status, stream, chain);
     // Split the outputs when the row chunks alone cannot fill the GPU, keeping
     // at least one output per warp in each split (every split re-stages and
     // re-slices the chunk's input rows).
@@ -756,9 +779,10 @@ cudaError_t launch_gf256_mxk(const MxkTask* tasks, const uint32_t* item_task, ui
     return cudaGetLastError();
 }
 
-cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream) {
-    if (gf16) return launch_single_impl<1>(task, status, grid, stream);
-    return launch_single_impl<0>(task, status, grid, stream);
+cudaError_t launch_mxk_single(const MxkTask& task, int gf16, int32_t* status, int grid, cudaStream_t stream,
+                              bool chain) {
+    if (gf16) return launch_single_impl<1>(task, status, grid, stream, chain);
+    return launch_single_impl<0>(task, status, grid, stream, chain);
 }
 
 cudaError_t launch_mxk_ksplit(const MxkTask& T, int gf16, int32_t* status, cudaStream_t stream) {
