@@ -259,10 +259,11 @@ __global__ void __launch_bounds__(1024) wht_pass_kernel(uint32_t* v, int lo, int
                                                         const uint8_t* known, const uint32_t* lw,
                                                         const uint16_t* exp16, uint16_t* values, uint16_t* derivs) {
     extern __shared__ uint32_t sv[];
-    pdl_trigger();  // after the last pass: the first transform pass may start slicing its rows
+    pdl_trigger();  // the next pass (or, after the last, the first transform pass) may start its set-up
     const uint32_t gsize = 1u << nb;
     const uint32_t gidx = blockIdx.x;
     const uint32_t base = ((gidx >> lo) << (lo + nb)) | (gidx & ((1u << lo) - 1u));
+    pdl_wait();  // v is the previous pass's output
     for (uint32_t t = threadIdx.x; t < gsize; t += blockDim.x) {
         const uint32_t i = base + (t << lo);
         sv[t] = in_mode ? (known[i] ? 0u : 1u) : v[i];
@@ -851,9 +852,20 @@ cudaError_t run_wht(uint32_t* v, uint32_t ts, int D, int in_mode, int out_mode, 
     for (int q = 0, lo = 0; q < n_pass; q++) {
         const int nb = (D - lo + (n_pass - q) - 1) / (n_pass - q);
         const uint32_t groups = ts >> nb, gsize = 1u << nb;
-        wht_pass_kernel<<<groups, std::min<uint32_t>(1024, std::max<uint32_t>(32, gsize / 2)), gsize * 4, st>>>(
-            v, lo, nb, q == 0 ? in_mode : 0, q + 1 == n_pass ? out_mode : 0, known, lw, exp16, values, derivs);
-        cudaError_t e = cudaGetLastError();
+        // chained after the pass before it (programmatic dependent launch);
+        // the locator's first pass follows the upload, a copy, and is plain
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(groups);
+        cfg.blockDim = dim3(std::min<uint32_t>(1024, std::max<uint32_t>(32, gsize / 2)));
+        cfg.dynamicSmemBytes = gsize * 4;
+        cfg.stream = st;
+        cfg.attrs = attr;
+        cfg.numAttrs = (q == 0 && in_mode) ? 0 : 1;
+        cudaError_t e = cudaLaunchKernelEx(&cfg, wht_pass_kernel, v, lo, nb, q == 0 ? in_mode : 0,
+                                           q + 1 == n_pass ? out_mode : 0, known, lw, exp16, values, derivs);
         if (e != cudaSuccess) return e;
         lo += nb;
     }
