@@ -356,14 +356,21 @@ __global__ void __launch_bounds__(128) derivative_kernel(const uint8_t* in, uint
     for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < total;
          x += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t j = (uint32_t)(x / G), g = (uint32_t)(x % G);
-        uint32_t acc[16];
+        uint32_t acc[16], cur[16], nxt[16];
 #pragma unroll
-        for (int t = 0; t < 16; t++) acc[t] = 0;
+        for (int t = 0; t < 16; t++) acc[t] = 0, cur[t] = 0, nxt[t] = 0;
+        // the partner row of bit b + 1 is loaded while bit b's product runs;
+        // b stays the same across the warp (the factor table jump is uniform)
+        auto fetch = [&](int b, uint32_t (&w)[16]) {
+            if (b < D && !((j >> b) & 1u)) load_planes(in + ((uint64_t)(j | (1u << b)) * G + g) * 64, w);
+        };
+        fetch(0, cur);
+#pragma unroll 1
         for (int b = 0; b < D; b++) {
-            if ((j >> b) & 1u) continue;
-            uint32_t w[16];
-            load_planes(in + ((uint64_t)(j | (1u << b)) * G + g) * 64, w);
-            mul16<true>(df.f[b], acc, w);
+            fetch(b + 1, nxt);
+            if (!((j >> b) & 1u)) mul16<true>(df.f[b], acc, cur);
+#pragma unroll
+            for (int t = 0; t < 16; t++) cur[t] = nxt[t];
         }
         store_planes(out + ((uint64_t)j * G + g) * 64, acc);
     }
